@@ -1,0 +1,323 @@
+"""Benchmark of the B200 Gross-Pitaevskii stepper.
+
+Workload (N = 1 line): 256^3 grid, periodic BCs, 4th-order centred FD, RK4
+dt = 0.005, eqn_to_solve = 2, seeded random-phase initial state, complex128
+storage and FP64 arithmetic.  One bench "step" = CHUNK (200) RK4 time steps
+of the whole grid.  Each field is 280 MB > L2 (126 MB), so no L2 flush is
+needed between steps.
+
+  value  site-updates/s with the state resident in HBM (CUDA events on the
+         solver's stream, max over ranks, summed over ranks' sites)
+  e2e    the same metric through the C ABI with host buffers: every bench
+         step copies psi in from pinned host memory (gpe_set_state), runs
+         CHUNK steps (gpe_step) and copies psi out (gpe_get_state)
+
+Multi-GPU (torchrun): every rank advances its own independent solve (replicas,
+weak scaling); there is no data-path collective.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "RK4 site-updates/s & HBM roofline %, 256^3; batched-solve p50/p99 latency"
+UNIT = "site-updates/s"
+CHUNK = 200
+WORKLOAD = dict(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
+                eqn_to_solve=2, bcs=1, order=4)
+CONFIG = {"workload": "256^3 periodic, 4th-order FD, RK4 dt=0.005, eqn 2, random-phase IC (seed 1234, kc 1.5), "
+                      "complex128", "grid": [256, 256, 256], "steps_per_bench_step": CHUNK,
+          "l2_policy": "inputs larger than L2 (each field 280 MB)", "parallelism": "replicas"}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_site(kind: str):
+    """DRAM bytes per site of one stage launch from the committed ncu
+    summary (profiles/), or None."""
+    f = ROOT / "profiles" / "ncu_rk4_stage_256cubed.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith(f"traffic_bytes_per_site[{kind}]"):
+            try:
+                return float(line.split("=")[1].split()[0])
+            except Exception:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(steps: int = 2):
+    """The reference's CPU path (C restatement in oracle/, OpenMP on all host
+    cores, per-call diss/Vtrap rebuild as the reference does) on a bounded
+    sample of the workload: `steps` RK4 steps of the 256^3 grid."""
+    from gpe_b200 import ic
+    from gpe_b200.solver import RunParams
+    from oracle.pyoracle import Oracle, load
+
+    lib = load()
+    cores = os.cpu_count() or 1
+    lib.or_set_threads(cores)
+    rp = RunParams(**WORKLOAD)
+    psi = ic.random_phase(rp, seed=1234, kc=1.5)
+    o = Oracle(rp)
+    o.faithful_cost(True)
+    o.run(psi, 1)  # first-touch / warm-up
+    t0 = time.perf_counter()
+    o.run(psi, steps)
+    dt = time.perf_counter() - t0
+    n = rp.nx * rp.ny * rp.nz
+    return {"value": n * steps / dt, "unit": UNIT, "cores": int(lib.or_get_threads()), "kind": "port",
+            "sample": f"{steps} RK4 steps of the 256^3 workload (C restatement of solve.f90/derivs.f90, "
+                      "reference binary unavailable: no Fortran compiler)"}
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's CPU implementation (oracle port) on
+    the host cores; rank 0 only."""
+    if rank != 0:
+        return 0
+    from gpe_b200 import ic
+    from gpe_b200.solver import RunParams
+    from oracle.pyoracle import Oracle, load
+
+    lib = load()
+    cores = os.cpu_count() or 1
+    lib.or_set_threads(cores)
+    rp = RunParams(**WORKLOAD)
+    psi = ic.random_phase(rp, seed=1234, kc=1.5)
+    o = Oracle(rp)
+    o.faithful_cost(True)
+    per = 1  # RK4 steps per bench step (bounded sample)
+    for _ in range(args.warmup):
+        psi = o.run(psi, per)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        psi = o.run(psi, per)
+    dt = time.perf_counter() - t0
+    n = rp.nx * rp.ny * rp.nz
+    v = n * per * args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(CONFIG, steps_per_bench_step=per), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": int(lib.or_get_threads()), "kind": "port",
+                             "sample": f"{per} RK4 step of the 256^3 workload per bench step; C restatement "
+                                       "of solve.f90/derivs.f90 (reference binary unavailable: no Fortran compiler)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from gpe_b200 import _lib as L
+    from gpe_b200 import ic
+    from gpe_b200.solver import RunParams, Solver
+
+    rp = RunParams(**WORKLOAD)
+    n_sites = rp.nx * rp.ny * rp.nz
+    psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
+    s = Solver(rp)
+    s.set_state(psi0)
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput -------------------------------------
+    for _ in range(args.warmup):
+        s.solver(CHUNK, wait=False)
+    s.sync()
+    s.lib.gpe_profile(s.h, 1)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            s.solver(CHUNK, wait=False)
+        ev1.record(stream)
+        s.sync()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = n_sites * CHUNK * args.steps * ws / (ms * 1e-3)
+    gpu_launches = 4 * CHUNK * args.steps
+
+    import ctypes as C
+
+    prof = {}
+    for kind, name in enumerate(L.KIND_NAMES):
+        tot, n, bps = C.c_double(), C.c_int64(), C.c_double()
+        s.lib.gpe_profile_get(s.h, kind, C.byref(tot), C.byref(n), C.byref(bps))
+        if n.value:
+            prof[name] = (tot.value, n.value, bps.value)
+    s.lib.gpe_profile(s.h, 0)
+
+    # roofline of the dominant kernel: the RK4 stage-2/3 kernel (80 B/site)
+    tot, n, bps = prof["rk4_23"]
+    avg_ms = tot / n
+    achieved = bps * n_sites / (avg_ms * 1e-3) / 1e9
+    peak, peak_src = measured_hbm_peak()
+    traffic_ps = ncu_traffic_per_site("rk4_23")
+    step_bytes = sum(v[2] * v[1] for v in prof.values()) * n_sites
+    step_ms = sum(v[0] for v in prof.values())
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (traffic_ps * n_sites) if traffic_ps else None,
+                "kernel": "k_stage<double2,double,R=2,RK4_2,TY=8> (RK4 stages 2 and 3)",
+                "bytes_per_site": bps, "avg_launch_ms": avg_ms, "peak_source": peak_src,
+                "frac_of_vendor_8000": achieved / 8000.0,
+                "all_stage_kernels_gbs": step_bytes / (step_ms * 1e-3) / 1e9,
+                "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()}}
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    host_in = torch.empty((rp.nz, rp.ny, rp.nx), dtype=torch.complex128, pin_memory=True)
+    host_in.numpy()[...] = psi0
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    hin, hout = host_in.numpy(), host_out.numpy()
+    for _ in range(1):
+        s.set_state(hin)
+        s.solver(CHUNK)
+        s.get_state(out=hout)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.set_state(hin)
+        s.solver(CHUNK)
+        s.get_state(out=hout)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ems = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": n_sites * CHUNK * args.steps * ws / (ems * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(hin.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
+           "ms_per_step": ems / args.steps}
+    gpu_launches += args.steps * (4 * CHUNK + 2)
+    assert np.isfinite(hout).all(), "non-finite state"
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+            "e2e": e2e, "roofline": roofline, "clocks": clk.summary(), "gpu_launches": gpu_launches}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    s.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

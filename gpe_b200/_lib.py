@@ -1,0 +1,109 @@
+"""ctypes binding of libgpe_cuda.so (include/gpe_cuda.h).
+
+The library is loaded from this package's lib/ directory only; there is no
+fallback implementation.  If the shared object is missing the import of the
+solver fails loudly with instructions to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgpe_cuda.so"
+
+GPE_OK = 0
+GPE_ERR_BADARG = -1
+GPE_ERR_CUDA = -2
+GPE_ERR_NONFINITE = -3
+GPE_ERR_TIMEOUT = -4
+GPE_ERR_NOMEM = -5
+GPE_ERR_NOMEM_BUDGET = -6
+GPE_ERR_STATE = -7
+
+GPE_EULER, GPE_RK2, GPE_RK4, GPE_RK45 = 0, 1, 2, 3
+GPE_C128, GPE_C64 = 0, 1
+GPE_COMPUTE_AUTO, GPE_COMPUTE_F32, GPE_COMPUTE_F64 = 0, 1, 2
+
+SCHEMES = {"euler": GPE_EULER, "rk2": GPE_RK2, "rk4": GPE_RK4, "rk45": GPE_RK45}
+
+
+class GpeParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("scheme", C.c_int32), ("eqn", C.c_int32), ("bcs", C.c_int32), ("order", C.c_int32),
+        ("real_time", C.c_int32), ("storage", C.c_int32), ("compute", C.c_int32),
+        ("xr", C.c_double), ("yr", C.c_double), ("zr", C.c_double),
+        ("tau", C.c_double),
+        ("Urhs", C.c_double), ("diss_amp", C.c_double), ("scal", C.c_double), ("g", C.c_double),
+        ("mu", C.c_double), ("nn", C.c_double), ("omx", C.c_double), ("omy", C.c_double),
+        ("omz", C.c_double), ("gamma", C.c_double),
+        ("eps", C.c_double), ("safety", C.c_double), ("dt_decrease", C.c_double),
+        ("dt_increase", C.c_double),
+    ]
+
+
+class GpeStepInfo(C.Structure):
+    _fields_ = [
+        ("t", C.c_double), ("im_t", C.c_double), ("dt_re", C.c_double), ("dt_im", C.c_double),
+        ("p", C.c_int64), ("accepted", C.c_int64), ("rejected", C.c_int64),
+        ("errmax", C.c_double), ("norm", C.c_double), ("energy", C.c_double),
+        ("want_norm", C.c_int32), ("want_energy", C.c_int32),
+    ]
+
+
+_PROTOS = {
+    "gpe_create": (C.c_int, [C.POINTER(GpeParams), C.POINTER(C.c_void_p)]),
+    "gpe_destroy": (None, [C.c_void_p]),
+    "gpe_last_error": (C.c_char_p, [C.c_void_p]),
+    "gpe_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_set_state_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_get_state_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(GpeStepInfo)]),
+    "gpe_step_async": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(GpeStepInfo)]),
+    "gpe_sync": (C.c_int, [C.c_void_p]),
+    "gpe_norm": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "gpe_energy": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "gpe_renormalise": (C.c_int, [C.c_void_p, C.c_double]),
+    "gpe_get_grid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gpe_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gpe_state_bytes": (C.c_int64, [C.POINTER(GpeParams)]),
+    "gpe_version": (C.c_char_p, []),
+    "gpe_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gpe_profile_get": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                  C.POINTER(C.c_double)]),
+}
+
+KIND_NAMES = ["euler", "rk2_1", "rk2_2", "rk4_1", "rk4_23", "rk4_4", "ck_1", "ck_2", "ck_3", "ck_4", "ck_5",
+              "ck_6", "energy"]
+
+_lib = None
+
+
+class GpeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gpe error {code}: {msg}")
+        self.code = code
+
+
+def load() -> C.CDLL:
+    """Load libgpe_cuda.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library with `python -m gpe_b200.build` "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_PROTOS)

@@ -1,0 +1,784 @@
+// C ABI of the B200 Gross-Pitaevskii time-stepper (include/gpe_cuda.h).
+//
+// One handle = one solve: ghost-padded device fields, per-axis tables, a
+// stream, reduction buffers.  gpe_step() enqueues one fused stage kernel per
+// Runge-Kutta stage; the time bookkeeping follows the reference's solver()
+// routines (src/solve.f90:57-244) on the host, in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpe_cuda.h"
+#include "gpe_aux.cuh"
+#include "gpe_device.cuh"
+
+namespace gpe {
+cudaError_t launch_stage_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
+cudaError_t launch_stage_f32(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
+cudaError_t launch_stage_f32x(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
+}  // namespace gpe
+
+using namespace gpe;
+
+namespace {
+
+thread_local std::string g_create_err;
+
+enum { CM_F64 = 0, CM_F32 = 1, CM_F32X = 2 };
+enum { T_VX, T_VY, T_VZ, T_SX, T_SY, T_SZ, T_WX, T_WY, T_WZ, T_CX, T_CY, T_CZ, T_NUM };
+
+// Cash-Karp tableau (src/solve.f90:255-269)
+const double CK_B[5][5] = {
+    {0.2, 0, 0, 0, 0},
+    {0.075, 0.225, 0, 0, 0},
+    {0.3, -0.9, 1.2, 0, 0},
+    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0},
+};
+
+}  // namespace
+
+struct gpe_handle {
+  gpe_params p{};
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  Geom g{};
+  int R = 2;
+  int esz = 16;
+  int cmode = CM_F64;
+  long long nelem = 0;  // padded elements per field
+  std::vector<void*> fields;
+  int cur = 0;  // index of the field holding psi
+  double* tables = nullptr;
+  std::vector<double> x, y, z;
+  double dx = 0, dy = 0, dz = 0;
+  double* part_a = nullptr;  // block partials (energy / first reduction)
+  double* part_b = nullptr;  // block partials (norm / errmax)
+  long long npart = 0;
+  double* dres = nullptr;    // [6] finalised reductions
+  double* hres = nullptr;    // pinned mirror of dres
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  int zc = 8;
+  dim3 grid;
+  std::string err;
+  // optional per-kernel timing (gpe_profile): event pairs around launches
+  bool prof = false;
+  std::vector<cudaEvent_t> ev;     // pool, 2 per launch
+  std::vector<int> ev_kind;        // kind of each pending pair
+  size_t ev_used = 0;              // pairs in flight
+  double prof_ms[K_NUM] = {0};
+  long long prof_n[K_NUM] = {0};
+};
+
+namespace {
+
+int fail(gpe_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_err = msg;
+  return code;
+}
+
+#define CU(h, call)                                                                        \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail((h), GPE_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + \
+                                         " at " #call);                                    \
+  } while (0)
+
+int validate(const gpe_params* p, std::string& why) {
+  if (!p) { why = "null parameters"; return GPE_ERR_BADARG; }
+  if (p->nx < 6 || p->ny < 6 || p->nz < 6) { why = "nx, ny, nz must be >= 6"; return GPE_ERR_BADARG; }
+  if (p->scheme < GPE_EULER || p->scheme > GPE_RK45) {
+    why = "ERROR: Unrecognised time stepping scheme.";  // src/solve.f90:49
+    return GPE_ERR_BADARG;
+  }
+  if (p->eqn < 1 || p->eqn > 4) { why = "eqn_to_solve must be 1..4"; return GPE_ERR_BADARG; }
+  if (p->bcs != 1 && p->bcs != 2) { why = "bcs must be 1 (periodic) or 2 (reflective)"; return GPE_ERR_BADARG; }
+  if (p->order != 2 && p->order != 4) { why = "order must be 2 or 4"; return GPE_ERR_BADARG; }
+  if (p->storage != GPE_C128 && p->storage != GPE_C64) { why = "storage must be GPE_C128 or GPE_C64"; return GPE_ERR_BADARG; }
+  if (!(p->xr > 0 && p->yr > 0 && p->zr > 0)) { why = "xr, yr, zr must be > 0"; return GPE_ERR_BADARG; }
+  if (!(p->tau > 0) || !std::isfinite(p->tau)) { why = "tau must be > 0"; return GPE_ERR_BADARG; }
+  return GPE_OK;
+}
+
+void layout(const gpe_params* p, Geom& g, int& esz) {
+  esz = p->storage == GPE_C128 ? 16 : 8;
+  g.nx = p->nx;
+  g.ny = p->ny;
+  g.nz = p->nz;
+  g.xoff = 128 / esz;
+  const long long need = g.xoff + (long long)p->nx + 2;
+  g.px = (need + g.xoff - 1) / g.xoff * g.xoff;
+  g.pz = (long long)(p->ny + 4) * g.px;
+}
+
+long long padded_elems(const Geom& g) { return (long long)(g.nz + 4) * g.pz; }
+
+int nfields(int scheme) {
+  switch (scheme) {
+    case GPE_EULER: return 2;
+    case GPE_RK2: return 2;
+    case GPE_RK4: return 4;
+    default: return 9;  // psi, psi_new, A, B, K1..K5
+  }
+}
+
+// z planes per block: enough blocks for several waves on 148 SMs
+int choose_zc(const Geom& g) {
+  if (const char* e = getenv("GPE_ZC")) {
+    int v = atoi(e);
+    if (v > 0) return std::min(v, g.nz);
+  }
+  const long long bxy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+  const long long target = 148LL * 2 * 6;
+  long long zc = (g.nz * bxy + target - 1) / target;
+  zc = std::max<long long>(4, std::min<long long>(zc, 64));
+  return (int)std::min<long long>(zc, g.nz);
+}
+
+cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a) {
+  switch (h->cmode) {
+    case CM_F64: return launch_stage_f64(kind, h->R, 8, h->grid, h->st, a);
+    case CM_F32: return launch_stage_f32(kind, h->R, 8, h->grid, h->st, a);
+    default: return launch_stage_f32x(kind, h->R, 8, h->grid, h->st, a);
+  }
+}
+
+cudaError_t launch(gpe_handle* h, int kind, const StageArgs& a) {
+  if (!h->prof) return launch_raw(h, kind, a);
+  if (2 * (h->ev_used + 1) > h->ev.size()) {
+    for (int q = 0; q < 64; ++q) {
+      cudaEvent_t e;
+      cudaError_t rc = cudaEventCreate(&e);
+      if (rc != cudaSuccess) return rc;
+      h->ev.push_back(e);
+    }
+  }
+  cudaEvent_t e0 = h->ev[2 * h->ev_used], e1 = h->ev[2 * h->ev_used + 1];
+  cudaEventRecord(e0, h->st);
+  cudaError_t rc = launch_raw(h, kind, a);
+  cudaEventRecord(e1, h->st);
+  if (h->ev_kind.size() <= h->ev_used) h->ev_kind.resize(h->ev_used + 1);
+  h->ev_kind[h->ev_used] = kind;
+  h->ev_used++;
+  return rc;
+}
+
+// after a stream synchronisation: fold the pending event pairs into totals
+void prof_resolve(gpe_handle* h) {
+  for (size_t q = 0; q < h->ev_used; ++q) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->ev[2 * q], h->ev[2 * q + 1]) == cudaSuccess) {
+      h->prof_ms[h->ev_kind[q]] += ms;
+      h->prof_n[h->ev_kind[q]] += 1;
+    }
+  }
+  h->ev_used = 0;
+}
+
+// algorithmic HBM traffic of one launch of a stage kind, in field elements
+// per site: one read of every input field and one write of every output
+// field (stencil neighbours come from on-chip reuse)
+int kind_elems(int kind) {
+  switch (kind) {
+    case K_EULER: return 2;
+    case K_RK2_1: return 2;
+    case K_RK2_2: return 3;
+    case K_RK4_1: return 3;
+    case K_RK4_2: return 5;
+    case K_RK4_4: return 3;
+    case K_CK_1: return 3;
+    case K_CK_2: return 5;
+    case K_CK_3: return 6;
+    case K_CK_4: return 7;
+    case K_CK_5: return 8;
+    case K_CK_6: return 7;
+    case K_ENERGY: return 1;
+    default: return 0;
+  }
+}
+
+// host tables and grid (src/ic.f90:32-69, solve.f90:397-409, ic.f90:713-731,
+// variables.f90:49-51 + 730-840)
+void build_tables(gpe_handle* h, std::vector<double>& t) {
+  const gpe_params& p = h->p;
+  const int n[3] = {p.nx, p.ny, p.nz};
+  const double r[3] = {p.xr, p.yr, p.zr};
+  const double om[3] = {p.omx, p.omy, p.omz};
+  std::vector<double>* c[3] = {&h->x, &h->y, &h->z};
+  double* d[3] = {&h->dx, &h->dy, &h->dz};
+  const double QC1 = 3.0 / 8.0, QC2 = 7.0 / 6.0, QC3 = 23.0 / 24.0;
+  const size_t ntot = (size_t)p.nx + p.ny + p.nz;
+  t.assign(ntot * 4, 0.0);
+  size_t off = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const double lo = -r[ax];
+    *d[ax] = (r[ax] - lo) / (n[ax] - 1);
+    c[ax]->resize(n[ax]);
+    for (int q = 0; q < n[ax]; ++q) (*c[ax])[q] = lo + (double)q * *d[ax];
+    const double a = (*c[ax])[n[ax] - 3];
+    for (int q = 0; q < n[ax]; ++q) {
+      const double xq = (*c[ax])[q];
+      t[0 * ntot + off + q] = (om[ax] * om[ax]) * (xq * xq);
+      t[1 * ntot + off + q] = 1.0 + tanh(xq - a) * tanh(xq + a);
+      double w = 1.0;
+      if (q == 0) w = QC1;
+      if (q == 1) w = QC2;
+      if (q == 2) w = QC3;
+      if (q == n[ax] - 3) w = QC3;
+      if (q == n[ax] - 2) w = QC2;
+      if (q == n[ax] - 1) w = QC1;
+      t[2 * ntot + off + q] = w;
+      t[3 * ntot + off + q] = xq;
+    }
+    off += n[ax];
+  }
+}
+
+StageArgs base_args(gpe_handle* h) {
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  const gpe_params& p = h->p;
+  a.g = h->g;
+  a.bcs = p.bcs;
+  a.eqn = p.eqn;
+  a.zc = h->zc;
+  a.has_urhs = (p.Urhs != 0.0) && p.eqn != 4;
+  a.has_diss = (p.diss_amp != 0.0) && (p.eqn == 1 || p.eqn == 3);
+  const double dx2 = h->dx * h->dx, dy2 = h->dy * h->dy, dz2 = h->dz * h->dz;
+  if (p.order == 2) {
+    a.ixx = 1.0 / dx2;
+    a.iyy = 1.0 / dy2;
+    a.izz = 1.0 / dz2;
+    a.ix1 = 1.0 / (2.0 * h->dx);
+  } else {
+    a.ixx = 1.0 / (12.0 * dx2);
+    a.iyy = 1.0 / (12.0 * dy2);
+    a.izz = 1.0 / (12.0 * dz2);
+    a.ix1 = 1.0 / (12.0 * h->dx);
+  }
+  a.g_nl = p.g;
+  a.mu = p.mu;
+  a.gamma = p.eqn == 4 ? p.gamma : 0.0;
+  a.urhs = p.Urhs;
+  a.diss_amp = p.diss_amp;
+  const size_t ntot = (size_t)p.nx + p.ny + p.nz;
+  const double* T = h->tables;
+  const double* blk[4] = {T, T + ntot, T + 2 * ntot, T + 3 * ntot};
+  a.vx = blk[0];
+  a.vy = blk[0] + p.nx;
+  a.vz = blk[0] + p.nx + p.ny;
+  a.sx = blk[1];
+  a.sy = blk[1] + p.nx;
+  a.sz = blk[1] + p.nx + p.ny;
+  a.wx = blk[2];
+  a.wy = blk[2] + p.nx;
+  a.wz = blk[2] + p.nx + p.ny;
+  a.cx = blk[3];
+  a.cy = blk[3] + p.nx;
+  a.cz = blk[3] + p.nx + p.ny;
+  return a;
+}
+
+int finalize_into(gpe_handle* h, const double* part, int slot) {
+  k_finalize<<<1, 256, 0, h->st>>>(part, h->npart, h->dres + 3 * slot);
+  CU(h, cudaGetLastError());
+  return GPE_OK;
+}
+
+int fetch_results(gpe_handle* h) {
+  CU(h, cudaMemcpyAsync(h->hres, h->dres, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  if (h->prof) prof_resolve(h);
+  return GPE_OK;
+}
+
+double rk_param(double v, double def) { return v != 0.0 ? v : def; }
+
+void default_dt(const gpe_params& p, gpe_step_info* io) {
+  if (io->dt_re == 0.0 && io->dt_im == 0.0) {
+    if (p.real_time) { io->dt_re = p.tau; io->dt_im = 0.0; }
+    else { io->dt_re = 0.0; io->dt_im = -p.tau; }
+  }
+}
+
+// One fixed-step step (Euler / RK2 / RK4) enqueued on the stream.
+int enqueue_fixed_step(gpe_handle* h, double dr, double di, bool energy, bool norm) {
+  StageArgs a = base_args(h);
+  void** F = h->fields.data();
+  const int sc = h->p.scheme;
+  if (sc == GPE_RK4) {
+    void *psi = F[0], *A = F[1], *B = F[2], *acc = F[3];
+    // s1: k1 = f(psi); A = psi + dt/2 k1; acc = psi + dt/6 k1
+    a.in = psi; a.out = A; a.acc = acc;
+    a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
+    a.cf_r[1] = dr / 6.0; a.cf_i[1] = di / 6.0;
+    a.want_energy = energy;
+    a.partials = energy ? h->part_a : nullptr;
+    CU(h, launch(h, K_RK4_1, a));
+    if (energy && finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
+    a.want_energy = 0;
+    a.partials = nullptr;
+    // s2: k2 = f(A); B = psi + dt/2 k2; acc += dt/3 k2
+    a.in = A; a.psi = psi; a.out = B;
+    a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
+    a.cf_r[1] = dr / 3.0; a.cf_i[1] = di / 3.0;
+    CU(h, launch(h, K_RK4_2, a));
+    // s3: k3 = f(B); A = psi + dt k3; acc += dt/3 k3
+    a.in = B; a.out = A;
+    a.cf_r[0] = dr; a.cf_i[0] = di;
+    CU(h, launch(h, K_RK4_2, a));
+    // s4: k4 = f(A); psi = acc + dt/6 k4
+    a.in = A; a.psi = nullptr; a.out = psi;
+    a.cf_r[0] = dr / 6.0; a.cf_i[0] = di / 6.0;
+    a.want_norm = norm;
+    a.partials = norm ? h->part_b : nullptr;
+    CU(h, launch(h, K_RK4_4, a));
+    if (norm && finalize_into(h, h->part_b, 1)) return GPE_ERR_CUDA;
+    return GPE_OK;
+  }
+  if (sc == GPE_RK2) {
+    void *psi = F[0], *A = F[1];
+    a.in = psi; a.out = A;
+    a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
+    a.want_energy = energy;
+    a.partials = energy ? h->part_a : nullptr;
+    CU(h, launch(h, K_RK2_1, a));
+    if (energy && finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
+    a.want_energy = 0;
+    a.in = A; a.psi = psi; a.out = psi;
+    a.cf_r[0] = dr; a.cf_i[0] = di;
+    a.want_norm = norm;
+    a.partials = norm ? h->part_b : nullptr;
+    CU(h, launch(h, K_RK2_2, a));
+    if (norm && finalize_into(h, h->part_b, 1)) return GPE_ERR_CUDA;
+    return GPE_OK;
+  }
+  // Euler: new = old + dt f(old), written into the other buffer
+  void *psi = F[h->cur], *nw = F[1 - h->cur];
+  a.in = psi; a.out = nw;
+  a.cf_r[0] = dr; a.cf_i[0] = di;
+  a.want_energy = energy;
+  a.want_norm = norm;
+  if (energy && !norm) {
+    a.partials = h->part_a;
+    CU(h, launch(h, K_EULER, a));
+    if (finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
+  } else {
+    a.partials = norm ? h->part_b : nullptr;
+    CU(h, launch(h, K_EULER, a));
+    if (norm && finalize_into(h, h->part_b, 1)) return GPE_ERR_CUDA;
+    // one kernel produced both sums: move the energy into its slot
+    if (energy) CU(h, cudaMemcpyAsync(h->dres + 1, h->dres + 4, sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  }
+  h->cur = 1 - h->cur;
+  return GPE_OK;
+}
+
+// RKF45 = rkqs (src/solve.f90:158-244) with Cash-Karp stages (248-378)
+int rk45_step(gpe_handle* h, gpe_step_info* io, bool energy, bool norm) {
+  const gpe_params& p = h->p;
+  const double eps = rk_param(p.eps, 1e-6), safety = rk_param(p.safety, 0.9);
+  const double dtdec = rk_param(p.dt_decrease, -0.25), dtinc = rk_param(p.dt_increase, -0.2);
+  const double errcon = pow(5.0 / safety, 1.0 / dtinc);
+  double dr = io->dt_re, di = io->dt_im;
+  const double dte_r = dr, dte_i = di;  // psi_scal uses the dt at entry (solve.f90:178)
+  void** F = h->fields.data();
+  void* psi = F[h->cur];
+  void* pnew = F[1 - h->cur];
+  void *A = F[2], *B = F[3];
+  void* K[5] = {F[4], F[5], F[6], F[7], F[8]};
+  double errmax = 0.0;
+  bool first = true;
+  for (int attempt = 0;; ++attempt) {
+    if (attempt > 10000) return fail(h, GPE_ERR_STATE, "rkqs: no acceptable step after 10000 attempts");
+    StageArgs a = base_args(h);
+    a.cf_r[0] = dr;
+    a.cf_i[0] = di;
+    a.psi = psi;
+    void* ins[6] = {psi, A, B, A, B, A};
+    void* outs[6] = {A, B, A, B, A, pnew};
+    for (int m = 0; m < 6; ++m) {
+      a.in = ins[m];
+      a.out = outs[m];
+      for (int q = 0; q < 5; ++q) a.b[q] = 0.0;
+      a.kout = m < 5 ? K[m] : nullptr;
+      if (m < 5) {
+        for (int q = 0; q <= m; ++q) a.b[q] = CK_B[m][q];
+        for (int q = 0; q < m; ++q) a.kin[q] = K[q];
+      } else {
+        a.kin[0] = K[0]; a.kin[1] = K[2]; a.kin[2] = K[3]; a.kin[3] = K[4];
+        a.dte_r = dte_r;
+        a.dte_i = dte_i;
+        a.inv_adt = 1.0 / hypot(dr, di);
+        a.want_norm = norm;
+      }
+      a.want_energy = (m == 0 && energy && first);
+      a.partials = (m == 5) ? h->part_b : (a.want_energy ? h->part_a : nullptr);
+      CU(h, launch(h, K_CK_1 + m, a));
+      if (a.want_energy && finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
+    }
+    if (finalize_into(h, h->part_b, 1)) return GPE_ERR_CUDA;
+    if (int rc = fetch_results(h)) return rc;
+    first = false;
+    errmax = h->hres[5] / eps;
+    if (!std::isfinite(errmax)) return fail(h, GPE_ERR_NONFINITE, "rkqs: non-finite error norm");
+    if (errmax <= 1.0) break;
+    io->rejected++;
+    const double e = pow(errmax, dtdec);
+    const double tr = (safety * dr) * e, ti = (safety * di) * e;
+    const double m = std::max(hypot(tr, ti), 0.1 * hypot(dr, di));
+    if (!p.real_time) { dr = 0.0; di = -m; }
+    else { dr = m; di = 0.0; }
+  }
+  double nr, ni;
+  if (errmax > errcon) {
+    const double e = pow(errmax, dtinc);
+    nr = (safety * dr) * e;
+    ni = (safety * di) * e;
+  } else {
+    nr = 5.0 * dr;
+    ni = 5.0 * di;
+  }
+  io->t = io->t + dr;
+  io->dt_re = nr;
+  io->dt_im = ni;
+  io->im_t = io->im_t + fabs(ni);  // the new dt, as src/solve.f90:229
+  io->errmax = errmax;
+  h->cur = 1 - h->cur;
+  return GPE_OK;
+}
+
+int norm_now(gpe_handle* h, double* out) {
+  const Geom& g = h->g;
+  const size_t ntot = (size_t)h->p.nx + h->p.ny + h->p.nz;
+  const double* w = h->tables + 2 * ntot;
+  if (h->esz == 16)
+    k_norm<double2><<<h->grid, dim3(32, 8), 0, h->st>>>((const double2*)h->fields[h->cur], g, h->zc, w, w + g.nx,
+                                                        w + g.nx + g.ny, h->part_b);
+  else
+    k_norm<float2><<<h->grid, dim3(32, 8), 0, h->st>>>((const float2*)h->fields[h->cur], g, h->zc, w, w + g.nx,
+                                                       w + g.nx + g.ny, h->part_b);
+  CU(h, cudaGetLastError());
+  if (int rc = finalize_into(h, h->part_b, 1)) return rc;
+  if (int rc = fetch_results(h)) return rc;
+  *out = ((h->hres[3] * h->dx) * h->dy) * h->dz;
+  return GPE_OK;
+}
+
+int ensure_staging(gpe_handle* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return GPE_OK;
+  if (h->staging) cudaFree(h->staging);
+  h->staging = nullptr;
+  h->staging_bytes = 0;
+  CU(h, cudaMalloc(&h->staging, bytes));
+  h->staging_bytes = bytes;
+  return GPE_OK;
+}
+
+int pack_from_device(gpe_handle* h, const void* src, int dtype) {
+  const int nb = 148 * 8;
+  void* dst = h->fields[h->cur];
+  if (h->esz == 16) {
+    if (dtype == GPE_C128) k_pack<double2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (double2*)dst, h->g, h->R, h->p.bcs);
+    else k_pack<double2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (double2*)dst, h->g, h->R, h->p.bcs);
+  } else {
+    if (dtype == GPE_C128) k_pack<float2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (float2*)dst, h->g, h->R, h->p.bcs);
+    else k_pack<float2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (float2*)dst, h->g, h->R, h->p.bcs);
+  }
+  CU(h, cudaGetLastError());
+  return GPE_OK;
+}
+
+int unpack_to_device(gpe_handle* h, void* dst, int dtype) {
+  const int nb = 148 * 8;
+  const void* src = h->fields[h->cur];
+  if (h->esz == 16) {
+    if (dtype == GPE_C128) k_unpack<double2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (double2*)dst, h->g);
+    else k_unpack<double2, float2><<<nb, 256, 0, h->st>>>((const double2*)src, (float2*)dst, h->g);
+  } else {
+    if (dtype == GPE_C128) k_unpack<float2, double2><<<nb, 256, 0, h->st>>>((const float2*)src, (double2*)dst, h->g);
+    else k_unpack<float2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (float2*)dst, h->g);
+  }
+  CU(h, cudaGetLastError());
+  return GPE_OK;
+}
+
+size_t interior_bytes(const gpe_handle* h, int dtype) {
+  return (size_t)h->p.nx * h->p.ny * h->p.nz * (dtype == GPE_C128 ? 16 : 8);
+}
+
+int check_dtype(gpe_handle* h, int dtype) {
+  if (dtype != GPE_C128 && dtype != GPE_C64) return fail(h, GPE_ERR_BADARG, "dtype must be GPE_C128 or GPE_C64");
+  return GPE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gpe_version(void) { return "gpe_b200 0.1 (sm_100a)"; }
+
+int64_t gpe_state_bytes(const gpe_params* p) {
+  std::string why;
+  if (validate(p, why)) return -1;
+  Geom g;
+  int esz;
+  layout(p, g, esz);
+  return (int64_t)padded_elems(g) * esz * nfields(p->scheme);
+}
+
+int gpe_create(const gpe_params* p, gpe_handle** out) {
+  if (!out) return fail(nullptr, GPE_ERR_BADARG, "null output handle pointer");
+  *out = nullptr;
+  std::string why;
+  if (int rc = validate(p, why)) return fail(nullptr, rc, why);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, GPE_ERR_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+  gpe_handle* h = new gpe_handle();
+  h->p = *p;
+  cudaGetDevice(&h->dev);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, h->dev) != cudaSuccess || prop.major < 10) {
+    delete h;
+    return fail(nullptr, GPE_ERR_CUDA, "an sm_100 (Blackwell) device is required");
+  }
+  layout(p, h->g, h->esz);
+  h->R = p->order / 2;
+  h->cmode = p->storage == GPE_C128 ? CM_F64 : (p->compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32);
+  h->nelem = padded_elems(h->g);
+  h->zc = choose_zc(h->g);
+  h->grid = dim3((p->nx + 31) / 32, (p->ny + 7) / 8, (p->nz + h->zc - 1) / h->zc);
+  h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
+  auto bail = [&](int rc) {
+    std::string m = h->err;
+    gpe_destroy(h);
+    return fail(nullptr, rc, m);
+  };
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    h->err = "cudaStreamCreate failed";
+    return bail(GPE_ERR_CUDA);
+  }
+  const int nf = nfields(p->scheme);
+  h->fields.assign(nf, nullptr);
+  for (int f = 0; f < nf; ++f) {
+    if (cudaMalloc(&h->fields[f], (size_t)h->nelem * h->esz) != cudaSuccess) {
+      cudaGetLastError();
+      h->err = "out of device memory allocating the solve's fields";
+      return bail(GPE_ERR_NOMEM);
+    }
+    cudaMemsetAsync(h->fields[f], 0, (size_t)h->nelem * h->esz, h->st);
+  }
+  std::vector<double> tab;
+  build_tables(h, tab);
+  if (cudaMalloc(&h->tables, tab.size() * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->part_a, h->npart * RED_SLOTS * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->part_b, h->npart * RED_SLOTS * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->dres, 6 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&h->hres, 6 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    h->err = "out of memory allocating tables / reduction buffers";
+    return bail(GPE_ERR_NOMEM);
+  }
+  cudaMemcpyAsync(h->tables, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, h->st);
+  cudaMemsetAsync(h->dres, 0, 6 * sizeof(double), h->st);
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h->err = "initialisation failed";
+    return bail(GPE_ERR_CUDA);
+  }
+  *out = h;
+  return GPE_OK;
+}
+
+void gpe_destroy(gpe_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->dev);
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (void* f : h->fields)
+    if (f) cudaFree(f);
+  if (h->tables) cudaFree(h->tables);
+  if (h->part_a) cudaFree(h->part_a);
+  if (h->part_b) cudaFree(h->part_b);
+  if (h->dres) cudaFree(h->dres);
+  if (h->hres) cudaFreeHost(h->hres);
+  if (h->staging) cudaFree(h->staging);
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+const char* gpe_last_error(const gpe_handle* h) { return h ? h->err.c_str() : g_create_err.c_str(); }
+
+int gpe_set_state(gpe_handle* h, const void* psi, int32_t dtype) {
+  if (!h || !psi) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  const size_t bytes = interior_bytes(h, dtype);
+  if (int rc = ensure_staging(h, bytes)) return rc;
+  CU(h, cudaMemcpyAsync(h->staging, psi, bytes, cudaMemcpyHostToDevice, h->st));
+  if (int rc = pack_from_device(h, h->staging, dtype)) return rc;
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_get_state(gpe_handle* h, void* psi, int32_t dtype) {
+  if (!h || !psi) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  const size_t bytes = interior_bytes(h, dtype);
+  if (int rc = ensure_staging(h, bytes)) return rc;
+  if (int rc = unpack_to_device(h, h->staging, dtype)) return rc;
+  CU(h, cudaMemcpyAsync(psi, h->staging, bytes, cudaMemcpyDeviceToHost, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_set_state_device(gpe_handle* h, const void* psi_dev, int32_t dtype) {
+  if (!h || !psi_dev) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  if (int rc = pack_from_device(h, psi_dev, dtype)) return rc;
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_get_state_device(gpe_handle* h, void* psi_dev, int32_t dtype) {
+  if (!h || !psi_dev) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  if (int rc = unpack_to_device(h, psi_dev, dtype)) return rc;
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+static int step_impl(gpe_handle* h, int64_t nsteps, gpe_step_info* io, bool wait) {
+  if (!h || !io || nsteps < 0) return fail(h, GPE_ERR_BADARG, "bad gpe_step arguments");
+  CU(h, cudaSetDevice(h->dev));
+  default_dt(h->p, io);
+  io->accepted = 0;
+  io->rejected = 0;
+  const bool want_e = io->want_energy != 0, want_n = io->want_norm != 0;
+  if (h->p.scheme == GPE_RK45) {
+    if (!wait) return fail(h, GPE_ERR_BADARG, "gpe_step_async does not support rk45");
+    for (int64_t s = 0; s < nsteps; ++s) {
+      if (int rc = rk45_step(h, io, want_e && s == 0, want_n && s == nsteps - 1)) return rc;
+      io->p += 1;
+      io->accepted += 1;
+    }
+  } else {
+    const double dr = io->dt_re, di = io->dt_im;
+    for (int64_t s = 0; s < nsteps; ++s) {
+      if (int rc = enqueue_fixed_step(h, dr, di, want_e && s == 0, want_n && s == nsteps - 1)) return rc;
+      io->t = io->t + dr;
+      io->im_t = io->im_t + fabs(di);
+      io->p += 1;
+      io->accepted += 1;
+    }
+    if (!wait) return GPE_OK;
+    if (int rc = fetch_results(h)) return rc;
+  }
+  if (want_e && nsteps > 0) io->energy = ((h->hres[1] * h->dx) * h->dy) * h->dz;
+  if (want_n && nsteps > 0) {
+    io->norm = ((h->hres[3] * h->dx) * h->dy) * h->dz;
+    if (!std::isfinite(io->norm)) return fail(h, GPE_ERR_NONFINITE, "non-finite norm: the solution blew up");
+  }
+  return GPE_OK;
+}
+
+int gpe_step(gpe_handle* h, int64_t nsteps, gpe_step_info* io) { return step_impl(h, nsteps, io, true); }
+
+int gpe_step_async(gpe_handle* h, int64_t nsteps, gpe_step_info* io) { return step_impl(h, nsteps, io, false); }
+
+int gpe_sync(gpe_handle* h) {
+  if (!h) return GPE_ERR_BADARG;
+  CU(h, cudaSetDevice(h->dev));
+  CU(h, cudaStreamSynchronize(h->st));
+  if (h->prof) prof_resolve(h);
+  return GPE_OK;
+}
+
+int gpe_profile(gpe_handle* h, int32_t enable) {
+  if (!h) return GPE_ERR_BADARG;
+  CU(h, cudaSetDevice(h->dev));
+  CU(h, cudaStreamSynchronize(h->st));
+  prof_resolve(h);
+  h->prof = enable != 0;
+  for (int k = 0; k < K_NUM; ++k) {
+    h->prof_ms[k] = 0.0;
+    h->prof_n[k] = 0;
+  }
+  return GPE_OK;
+}
+
+int gpe_profile_get(gpe_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes_per_site) {
+  if (!h || kind < 0 || kind >= K_NUM) return fail(h, GPE_ERR_BADARG, "bad profile kind");
+  CU(h, cudaSetDevice(h->dev));
+  CU(h, cudaStreamSynchronize(h->st));
+  prof_resolve(h);
+  if (total_ms) *total_ms = h->prof_ms[kind];
+  if (launches) *launches = h->prof_n[kind];
+  if (bytes_per_site) *bytes_per_site = (double)kind_elems(kind) * h->esz;
+  return GPE_OK;
+}
+
+int gpe_norm(gpe_handle* h, double* norm) {
+  if (!h || !norm) return fail(h, GPE_ERR_BADARG, "null argument");
+  CU(h, cudaSetDevice(h->dev));
+  return norm_now(h, norm);
+}
+
+int gpe_energy(gpe_handle* h, double* energy) {
+  if (!h || !energy) return fail(h, GPE_ERR_BADARG, "null argument");
+  CU(h, cudaSetDevice(h->dev));
+  StageArgs a = base_args(h);
+  a.in = h->fields[h->cur];
+  a.want_energy = 1;
+  a.partials = h->part_a;
+  CU(h, launch(h, K_ENERGY, a));
+  if (int rc = finalize_into(h, h->part_a, 0)) return rc;
+  if (int rc = fetch_results(h)) return rc;
+  *energy = ((h->hres[1] * h->dx) * h->dy) * h->dz;
+  return GPE_OK;
+}
+
+int gpe_renormalise(gpe_handle* h, double norm) {
+  if (!h || !(norm > 0)) return fail(h, GPE_ERR_BADARG, "norm must be > 0");
+  CU(h, cudaSetDevice(h->dev));
+  const double a = sqrt(h->p.nn), b = sqrt(norm);
+  if (h->esz == 16) k_scale<double2><<<148 * 8, 256, 0, h->st>>>((double2*)h->fields[h->cur], h->nelem, a, b);
+  else k_scale<float2><<<148 * 8, 256, 0, h->st>>>((float2*)h->fields[h->cur], h->nelem, a, b);
+  CU(h, cudaGetLastError());
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_get_grid(const gpe_handle* h, double* x, double* y, double* z, double* dxyz) {
+  if (!h) return GPE_ERR_BADARG;
+  if (x) memcpy(x, h->x.data(), sizeof(double) * h->x.size());
+  if (y) memcpy(y, h->y.data(), sizeof(double) * h->y.size());
+  if (z) memcpy(z, h->z.data(), sizeof(double) * h->z.size());
+  if (dxyz) {
+    dxyz[0] = h->dx;
+    dxyz[1] = h->dy;
+    dxyz[2] = h->dz;
+  }
+  return GPE_OK;
+}
+
+int gpe_get_stream(const gpe_handle* h, void** stream) {
+  if (!h || !stream) return GPE_ERR_BADARG;
+  *stream = (void*)h->st;
+  return GPE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,510 @@
+// Device side of the B200 Gross-Pitaevskii stepper: the fused RK stage
+// kernel (stencil + GP right-hand side + stage combination + reductions).
+//
+// Reference path restated here (anthonyyoud/gpe):
+//   src/derivs.f90:25-64, 146-272   2nd/4th order centred differences
+//   src/derivs.f90:276-398          boundary index maps (see ghost_pos)
+//   src/variables.f90:55-71         laplacian = dxx + dyy + dzz
+//   src/solve.f90:382-440           get_rhs, equations 1-4
+//   src/solve.f90:57-378            Euler / RK2 / RK4 / Cash-Karp stages
+//   src/variables.f90:554-604       get_norm, energy
+//
+// HBM layout (one solve, one field): a ghost-padded array
+//   elem(i,j,k) = (k+2)*pz + (j+2)*px + XOFF + i,
+//   i in [-2, nx+1], j in [-2, ny+1], k in [-2, nz+1],
+// with XOFF = 128 B / sizeof(element) so that x = 0 of every row starts on a
+// 128-byte boundary and px a multiple of XOFF.  The producer of every field
+// that is read through the stencil writes, next to each interior value, the
+// face ghosts that the boundary conditions map onto it; the stencil then has
+// no boundary logic at all.  Periodic and reflective BCs differ only in
+// where the producer writes ghosts.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gpe {
+
+enum StageKind : int {
+  K_EULER = 0,
+  K_RK2_1,
+  K_RK2_2,
+  K_RK4_1,
+  K_RK4_2,  // also used for RK4 stage 3 (same data flow, other coefficient)
+  K_RK4_4,
+  K_CK_1,
+  K_CK_2,
+  K_CK_3,
+  K_CK_4,
+  K_CK_5,
+  K_CK_6,
+  K_ENERGY,  // no stores: energy of the input state only
+  K_NUM
+};
+
+// reduction slots in the per-block partials: [norm, energy, errmax]
+enum { RED_NORM = 0, RED_ENERGY = 1, RED_ERR = 2, RED_SLOTS = 3 };
+
+struct Geom {
+  int nx, ny, nz;
+  int xoff;             // elements before x = 0 in a row
+  long long px, pz;     // row and plane pitch in elements
+};
+
+struct StageArgs {
+  Geom g;
+  int bcs;              // 1 periodic, 2 reflective
+  int eqn;              // 1..4
+  int zc;               // z planes per block
+  int want_norm, want_energy;
+  int has_urhs, has_diss;
+  const void* in;       // stencil input (ghost-padded)
+  const void* psi;      // psi_n, read point-wise
+  void* acc;            // RK4 accumulator (read/write point-wise)
+  void* out;            // stencil output for the next stage (+ ghosts)
+  void* kout;           // Cash-Karp: K_m = dt*f for this stage
+  const void* kin[5];   // Cash-Karp: K_1..K_{m-1}
+  double cf_r[2], cf_i[2];  // complex stage coefficients
+  double b[6];              // real Cash-Karp coefficients of this stage
+  double dte_r, dte_i;      // dt at entry of rkqs (psi_scal)
+  double inv_adt;           // 1/|dt| of this attempt (psi_scal)
+  // stencil constants
+  double ixx, iyy, izz;     // 1/dx2 (order 2) or 1/(12 dx2) (order 4)
+  double ix1;               // 1/(2dx) (order 2) or 1/(12dx) (order 4)
+  double g_nl, mu, gamma, urhs, diss_amp;
+  // per-axis tables, length n of each axis
+  const double *vx, *vy, *vz;   // om^2 x^2 (Vtrap pieces)
+  const double *sx, *sy, *sz;   // 1 + tanh(x-a)tanh(x+a) (diss pieces)
+  const double *wx, *wy, *wz;   // norm quadrature weights
+  const double *cx, *cy, *cz;   // coordinates (sphere)
+  double* partials;             // [nblocks][RED_SLOTS]
+};
+
+template <class S>
+struct Stor;
+template <>
+struct Stor<double2> {
+  using R = double;
+  static constexpr int XOFF = 8;
+};
+template <>
+struct Stor<float2> {
+  using R = float;
+  static constexpr int XOFF = 16;
+};
+
+template <class C>
+struct cx {
+  C r, i;
+};
+
+template <class C, class S>
+__device__ __forceinline__ cx<C> to_c(const S& v) {
+  return cx<C>{(C)v.x, (C)v.y};
+}
+template <class S, class C>
+__device__ __forceinline__ S to_s(const cx<C>& v) {
+  S s;
+  s.x = (typename Stor<S>::R)v.r;
+  s.y = (typename Stor<S>::R)v.i;
+  return s;
+}
+template <class S>
+__device__ __forceinline__ S szero() {
+  S s;
+  s.x = 0;
+  s.y = 0;
+  return s;
+}
+
+// Read-only, non-coherent global load for inputs no thread writes in the
+// same launch.
+template <class S>
+__device__ __forceinline__ S ldro(const S* p) {
+  return __ldg(p);
+}
+
+constexpr int NOGHOST = -1000000;
+
+// Ghost position written next to interior index q of an axis with n points,
+// stencil radius R (derivs.f90:276-398 restated as ghost cells):
+//   periodic:   ghost(q+n) = psi(q) for q < R;  ghost(q-n) = psi(q) for q >= n-R
+//   reflective: ghost(-q) = psi(q) for 1 <= q <= R;
+//               ghost(2(n-1)-q) = psi(q) for n-1-R <= q <= n-2
+// (even mirror about the end node: x_{-1} = x_1, x_{n+1} = x_{n-1}).
+// For n >= 6 at most one ghost exists per axis.
+__host__ __device__ __forceinline__ int ghost_pos(int q, int n, int R, int bcs) {
+  if (bcs == 1) {
+    if (q < R) return q + n;
+    if (q >= n - R) return q - n;
+  } else {
+    if (q >= 1 && q <= R) return -q;
+    if (q >= n - 1 - R && q <= n - 2) return 2 * (n - 1) - q;
+  }
+  return NOGHOST;
+}
+
+// 2nd derivative along one axis, expression order of derivs.f90:164-181
+template <class C, int R>
+__device__ __forceinline__ cx<C> d2(cx<C> m2, cx<C> m1, cx<C> c0, cx<C> p1, cx<C> p2, C inv) {
+  cx<C> o;
+  if constexpr (R == 1) {
+    o.r = ((p1.r - (C)2 * c0.r) + m1.r) * inv;
+    o.i = ((p1.i - (C)2 * c0.i) + m1.i) * inv;
+  } else {
+    o.r = ((((-p2.r + (C)16 * p1.r) - (C)30 * c0.r) + (C)16 * m1.r) - m2.r) * inv;
+    o.i = ((((-p2.i + (C)16 * p1.i) - (C)30 * c0.i) + (C)16 * m1.i) - m2.i) * inv;
+  }
+  return o;
+}
+
+// 1st derivative (derivs.f90:43, 54-57)
+template <class C, int R>
+__device__ __forceinline__ cx<C> d1(cx<C> m2, cx<C> m1, cx<C> p1, cx<C> p2, C inv) {
+  cx<C> o;
+  if constexpr (R == 1) {
+    o.r = (p1.r - m1.r) * inv;
+    o.i = (p1.i - m1.i) * inv;
+  } else {
+    o.r = (((-p2.r + (C)8 * p1.r) - (C)8 * m1.r) + m2.r) * inv;
+    o.i = (((-p2.i + (C)8 * p1.i) - (C)8 * m1.i) + m2.i) * inv;
+  }
+  return o;
+}
+
+// GP right-hand side at one site (solve.f90:414-437)
+// vxy = vx[i] + vy[j] and sxy = sx[i] + sy[j] are hoisted out of the z loop;
+// the sums keep the reference's left-to-right order.
+template <class C>
+__device__ __forceinline__ cx<C> gp_rhs(const StageArgs& a, cx<C> p, cx<C> lap, cx<C> dpx, double vxy,
+                                        double sxy, int i, int j, int k) {
+  cx<C> r;
+  const C n2 = p.r * p.r + p.i * p.i;
+  if (a.eqn == 4) {
+    // -(i + gamma) * (-0.5 lap + V psi + g |psi|^2 psi - mu psi)
+    const C v = (C)(0.5 * (vxy + a.vz[k]));
+    const C g = (C)a.g_nl, mu = (C)a.mu;
+    const C wr = ((-(C)0.5 * lap.r + v * p.r) + g * (n2 * p.r)) - mu * p.r;
+    const C wi = ((-(C)0.5 * lap.i + v * p.i) + g * (n2 * p.i)) - mu * p.i;
+    const C gm = (C)a.gamma;
+    r.r = wi - gm * wr;
+    r.i = -wr - gm * wi;
+  } else if (a.eqn == 2) {
+    // i (lap - |psi|^2 psi) + U dpsi/dx
+    const C cr = lap.r - n2 * p.r, ci = lap.i - n2 * p.i;
+    r.r = -ci;
+    r.i = cr;
+    if (a.has_urhs) {
+      r.r += (C)a.urhs * dpx.r;
+      r.i += (C)a.urhs * dpx.i;
+    }
+  } else {
+    // 0.5 (i + diss) (lap + (1 - |psi|^2) psi) + U dpsi/dx   [eqn 3: * sphere]
+    const C s = (C)1 - n2;
+    const C cr = lap.r + s * p.r, ci = lap.i + s * p.i;
+    C dd = 0;
+    if (a.has_diss) dd = (C)(0.5 * (a.diss_amp * (sxy + a.sz[k])));
+    r.r = dd * cr - (C)0.5 * ci;
+    r.i = dd * ci + (C)0.5 * cr;
+    if (a.has_urhs) {
+      r.r += (C)a.urhs * dpx.r;
+      r.i += (C)a.urhs * dpx.i;
+    }
+    if (a.eqn == 3) {
+      const double xx = a.cx[i], yy = a.cy[j], zz = a.cz[k];
+      const C sp = (C)(0.5 * (1.0 + tanh((sqrt((xx * xx + yy * yy) + zz * zz) - 10.0) - 2.0)));
+      r.r *= sp;
+      r.i *= sp;
+    }
+  }
+  return r;
+}
+
+__device__ __forceinline__ cx<double> cmuld(double ar, double ai, cx<double> b) {
+  return cx<double>{ar * b.r - ai * b.i, ar * b.i + ai * b.r};
+}
+
+// Store v at interior (i,j,k) of a ghost-padded field and at its face ghosts.
+template <class S>
+__device__ __forceinline__ void store_with_ghosts(S* f, const Geom& g, long long col, int i, int j, int k, int gx,
+                                                  int gy, int gz, S v) {
+  const long long pl = (long long)(k + 2) * g.pz;
+  f[pl + col] = v;
+  if (gx != NOGHOST) f[pl + (long long)(j + 2) * g.px + g.xoff + gx] = v;
+  if (gy != NOGHOST) f[pl + (long long)(gy + 2) * g.px + g.xoff + i] = v;
+  if (gz != NOGHOST) f[(long long)(gz + 2) * g.pz + col] = v;
+}
+
+// Deterministic block sum of up to RED_SLOTS values (fixed shuffle and warp
+// order), thread 0 writes the block's partials.  Slot RED_ERR is a max.
+template <int NT>
+__device__ __forceinline__ void block_reduce_store(double v0, double v1, double v2, double* partials) {
+  __shared__ double red[NT / 32][RED_SLOTS];
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_down_sync(0xffffffffu, v0, o);
+    v1 += __shfl_down_sync(0xffffffffu, v1, o);
+    v2 = fmax(v2, __shfl_down_sync(0xffffffffu, v2, o));
+  }
+  if ((tid & 31) == 0) {
+    red[tid >> 5][0] = v0;
+    red[tid >> 5][1] = v1;
+    red[tid >> 5][2] = v2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int w = 0; w < NT / 32; ++w) {
+      s0 += red[w][0];
+      s1 += red[w][1];
+      s2 = fmax(s2, red[w][2]);
+    }
+    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    partials[b * RED_SLOTS + 0] = s0;
+    partials[b * RED_SLOTS + 1] = s1;
+    partials[b * RED_SLOTS + 2] = s2;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel.
+//
+// Block = 32 (x) x TY (y) threads owning an x-y tile and marching over zc
+// planes in z.  Per plane: the centre plane's tile plus a radius-R halo sits
+// in shared memory (x and y neighbours); the z neighbours of each column sit
+// in a register queue of 2R+1 values.  The next plane of the queue and the
+// next halo are prefetched one iteration ahead, so every element of the
+// stencil input is read from HBM about once per stage; halo re-reads hit L2.
+// ---------------------------------------------------------------------------
+template <class S, class C, int R, int KIND, int TY>
+__global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
+  constexpr int TX = 32, NT = TX * TY;
+  constexpr int TW = TX + 2 * R, TH = TY + 2 * R;
+  constexpr int NH = 2 * R * TX + 2 * R * TY;  // halo points per plane
+  constexpr int HPT = (NH + NT - 1) / NT;      // halo points per thread
+  constexpr bool HAS_PSI = (KIND == K_RK2_2 || KIND == K_RK4_2 || (KIND >= K_CK_2 && KIND <= K_CK_6));
+  constexpr bool HAS_ACC = (KIND == K_RK4_2 || KIND == K_RK4_4);
+  // Cash-Karp K inputs: stages 2..5 read K_1..K_{m-1}; stage 6 reads K1, K3,
+  // K4, K5 (K2 only enters with the zero weights c2 = dc2 = 0).
+  constexpr int NK = (KIND >= K_CK_2 && KIND <= K_CK_5) ? (KIND - K_CK_1) : (KIND == K_CK_6 ? 4 : 0);
+
+  __shared__ S tile[TH * TW];
+
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i = blockIdx.x * TX + tx;
+  const int j = blockIdx.y * TY + ty;
+  const int kb = blockIdx.z * a.zc;
+  const int ke = min(kb + a.zc, g.nz);
+  const bool ldok = (i <= g.nx + 1) && (j <= g.ny + 1);
+  const bool active = (i < g.nx) && (j < g.ny);
+  const long long col = (long long)(j + 2) * g.px + g.xoff + i;
+  const S* __restrict__ in = (const S*)a.in;
+
+  // halo bookkeeping
+  long long hcol[HPT];
+  int hsm[HPT];
+  bool hok[HPT];
+#pragma unroll
+  for (int h = 0; h < HPT; ++h) {
+    const int p = tid + h * NT;
+    int hy = 0, hx = 0;
+    if (p < 2 * R * TX) {
+      const int r = p / TX, c = p % TX;
+      hy = r < R ? r : TY + r;
+      hx = R + c;
+    } else {
+      const int q = p - 2 * R * TX;
+      const int r = q / (2 * R), c = q % (2 * R);
+      hy = R + r;
+      hx = c < R ? c : TX + c;
+    }
+    const int gi = blockIdx.x * TX + hx - R, gj = blockIdx.y * TY + hy - R;
+    hok[h] = (p < NH) && gi >= -2 && gi <= g.nx + 1 && gj >= -2 && gj <= g.ny + 1;
+    hsm[h] = (p < NH) ? hy * TW + hx : 0;
+    hcol[h] = (long long)(gj + 2) * g.px + g.xoff + gi;
+  }
+
+  const int gx = ghost_pos(i, g.nx, R, a.bcs);
+  const int gy = ghost_pos(j, g.ny, R, a.bcs);
+  const double wxy = active ? a.wx[i] * a.wy[j] : 0.0;
+  const double vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
+  const double sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
+
+  // z queue and halo of the first plane
+  S q[2 * R + 1];
+#pragma unroll
+  for (int d = 0; d <= 2 * R; ++d) q[d] = ldok ? ldro(in + (long long)(kb - R + d + 2) * g.pz + col) : szero<S>();
+  S hv[HPT];
+#pragma unroll
+  for (int h = 0; h < HPT; ++h) hv[h] = hok[h] ? ldro(in + (long long)(kb + 2) * g.pz + hcol[h]) : szero<S>();
+
+  // point-wise inputs of the first plane
+  const S* psi = (const S*)a.psi;
+  S* acc = (S*)a.acc;
+  S pv = szero<S>(), av = szero<S>();
+  S kv[NK > 0 ? NK : 1];
+  if (active) {
+    const long long o = (long long)(kb + 2) * g.pz + col;
+    if constexpr (HAS_PSI) pv = ldro(psi + o);
+    if constexpr (HAS_ACC) av = acc[o];
+#pragma unroll
+    for (int m = 0; m < NK; ++m) kv[m] = ldro((const S*)a.kin[m] + o);
+  }
+
+  double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+
+  for (int k = kb; k < ke; ++k) {
+    const bool more = (k + 1 < ke);
+    // prefetch the next iteration's loads
+    S qn = szero<S>();
+    S hn[HPT];
+    S pn = szero<S>(), an = szero<S>();
+    S kn[NK > 0 ? NK : 1];
+    if (more) {
+      if (ldok) qn = ldro(in + (long long)(k + R + 3) * g.pz + col);
+#pragma unroll
+      for (int h = 0; h < HPT; ++h) hn[h] = hok[h] ? ldro(in + (long long)(k + 3) * g.pz + hcol[h]) : szero<S>();
+      if (active) {
+        const long long o = (long long)(k + 3) * g.pz + col;
+        if constexpr (HAS_PSI) pn = ldro(psi + o);
+        if constexpr (HAS_ACC) an = acc[o];
+#pragma unroll
+        for (int m = 0; m < NK; ++m) kn[m] = ldro((const S*)a.kin[m] + o);
+      }
+    }
+
+    __syncthreads();
+    tile[(ty + R) * TW + tx + R] = q[R];
+#pragma unroll
+    for (int h = 0; h < HPT; ++h)
+      if (tid + h * NT < NH) tile[hsm[h]] = hv[h];
+    __syncthreads();
+
+    if (active) {
+      const int ts = (ty + R) * TW + tx + R;
+      const cx<C> c0 = to_c<C>(q[R]);
+      cx<C> xm2{0, 0}, xp2{0, 0}, ym2{0, 0}, yp2{0, 0}, zm2{0, 0}, zp2{0, 0};
+      const cx<C> xm1 = to_c<C>(tile[ts - 1]), xp1 = to_c<C>(tile[ts + 1]);
+      const cx<C> ym1 = to_c<C>(tile[ts - TW]), yp1 = to_c<C>(tile[ts + TW]);
+      const cx<C> zm1 = to_c<C>(q[R - 1]), zp1 = to_c<C>(q[R + 1]);
+      if constexpr (R == 2) {
+        xm2 = to_c<C>(tile[ts - 2]);
+        xp2 = to_c<C>(tile[ts + 2]);
+        ym2 = to_c<C>(tile[ts - 2 * TW]);
+        yp2 = to_c<C>(tile[ts + 2 * TW]);
+        zm2 = to_c<C>(q[0]);
+        zp2 = to_c<C>(q[4]);
+      }
+      const cx<C> lxx = d2<C, R>(xm2, xm1, c0, xp1, xp2, (C)a.ixx);
+      const cx<C> lyy = d2<C, R>(ym2, ym1, c0, yp1, yp2, (C)a.iyy);
+      const cx<C> lzz = d2<C, R>(zm2, zm1, c0, zp1, zp2, (C)a.izz);
+      cx<C> lap;
+      lap.r = (lxx.r + lyy.r) + lzz.r;
+      lap.i = (lxx.i + lyy.i) + lzz.i;
+
+      const int gz = ghost_pos(k, g.nz, R, a.bcs);
+      const long long o = (long long)(k + 2) * g.pz + col;
+      const double cr = (double)c0.r, ci = (double)c0.i;
+
+      if constexpr (KIND == K_ENERGY || KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_CK_1) {
+        if (a.want_energy) {
+          // real(-lap * conjg(psi) + 0.5 |psi|^4)   (variables.f90:591-592)
+          const double n2 = cr * cr + ci * ci;
+          r_en += (-(double)lap.r * cr - (double)lap.i * ci) + 0.5 * (n2 * n2);
+        }
+      }
+
+      if constexpr (KIND != K_ENERGY) {
+        cx<C> dpx{0, 0};
+        if (a.has_urhs) dpx = d1<C, R>(xm2, xm1, xp1, xp2, (C)a.ix1);
+        const cx<C> f = gp_rhs<C>(a, c0, lap, dpx, vxy, sxy, i, j, k);
+        const cx<double> fd{(double)f.r, (double)f.i};
+        S* out = (S*)a.out;
+
+        if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 ||
+                      KIND == K_RK4_2 || KIND == K_RK4_4) {
+          // out = base + cf0 * f
+          cx<double> base;
+          if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
+          else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
+          else base = cx<double>{cr, ci};
+          const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
+          const cx<double> nv{base.r + t0.r, base.i + t0.i};
+          const S ns = to_s<S>(nv);
+          store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, ns);
+          if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
+            // acc = (psi | acc) + cf1 * f
+            const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
+            const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
+            acc[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
+          }
+          if constexpr (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4) {
+            if (a.want_norm) {
+              const double sr = (double)ns.x, si = (double)ns.y;
+              r_norm += (wxy * a.wz[k]) * (sr * sr + si * si);
+            }
+          }
+        } else {
+          // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
+          const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
+          const S Ks = to_s<S>(Km);
+          const cx<double> Kmd = to_c<double>(Ks);
+          const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
+          if constexpr (KIND != K_CK_6) {
+            ((S*)a.kout)[o] = Ks;
+            double tr = pd.r, ti = pd.i;
+#pragma unroll
+            for (int m = 0; m < NK; ++m) {
+              const cx<double> km = to_c<double>(kv[m]);
+              tr = tr + a.b[m] * km.r;
+              ti = ti + a.b[m] * km.i;
+            }
+            tr = tr + a.b[NK] * Kmd.r;
+            ti = ti + a.b[NK] * Kmd.i;
+            store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, to_s<S>(cx<double>{tr, ti}));
+          } else {
+            // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
+            // contribute exact zeros and are skipped.
+            const cx<double> k1 = to_c<double>(kv[0]), k3 = to_c<double>(kv[1]);
+            const cx<double> k4 = to_c<double>(kv[2]), k5 = to_c<double>(kv[3]);
+            const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
+            const double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0;
+            const double DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0, DC6 = C6 - 0.25;
+            const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
+            const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
+            const S ns = to_s<S>(cx<double>{nr, ni});
+            store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, ns);
+            const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
+            const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
+            // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
+            const double fa = hypot(k1.r, k1.i) * a.inv_adt;
+            const double sr = (hypot(pd.r, pd.i) + a.dte_r * fa) + 1e-30;
+            const double si = a.dte_i * fa;
+            const double ratio = hypot(er, ei) / hypot(sr, si);
+            r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
+            if (a.want_norm) {
+              const double qr = (double)ns.x, qi = (double)ns.y;
+              r_norm += (wxy * a.wz[k]) * (qr * qr + qi * qi);
+            }
+          }
+        }
+      }
+    }
+
+    // rotate the queue
+#pragma unroll
+    for (int d = 0; d < 2 * R; ++d) q[d] = q[d + 1];
+    q[2 * R] = qn;
+#pragma unroll
+    for (int h = 0; h < HPT; ++h) hv[h] = hn[h];
+    pv = pn;
+    av = an;
+#pragma unroll
+    for (int m = 0; m < NK; ++m) kv[m] = kn[m];
+  }
+
+  if (a.partials) block_reduce_store<NT>(r_norm, r_en, r_err, a.partials);
+}
+
+}  // namespace gpe

@@ -1,0 +1,196 @@
+"""Python host interface of the B200 stepper, mirroring the reference's
+solver interface (anthonyyoud/gpe):
+
+    call solver(psi%old, psi%new)   -> Solver.solver(nsteps)      (src/solve.f90:25)
+    call get_norm(psi, norm)        -> Solver.get_norm()          (src/variables.f90:554)
+    call energy(psi, E)             -> Solver.energy()            (src/variables.f90:580)
+    call renormalise(psi, norm)     -> Solver.renormalise(norm)   (src/variables.f90:715)
+    call get_grid()                 -> Solver.grid()              (src/ic.f90:32)
+
+The globals of src/parameters.f90 (t, im_t, dt, p) live on the Solver and
+are advanced by solver() exactly as the reference's routines advance them.
+Arrays are numpy complex128/complex64 of shape (nz, ny, nx) in C order,
+which is the reference's psi(0:nx-1,0:ny-1,0:nz-1) memory layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class RunParams:
+    """run.in / parameters.in quantities the stepper needs
+    (src/parameters.f90:24-56, src/parameters.in:22-30)."""
+    nx: int = 64
+    ny: int = 64
+    nz: int = 64
+    xr: float = 16.0
+    yr: float = 16.0
+    zr: float = 16.0
+    tau: float = 0.01
+    scheme: str = "rk4"
+    eqn_to_solve: int = 4
+    bcs: int = 2
+    order: int = 2
+    real_time: bool = True
+    Urhs: float = 0.0
+    diss_amp: float = 0.0
+    scal: float = 1.0
+    g: float = 1.0
+    mu: float = 1.0
+    nn: float = 1.0
+    omx: float = 0.0
+    omy: float = 0.0
+    omz: float = 0.0
+    gamma: float = 0.0
+    storage: str = "c128"      # "c128" | "c64"
+    compute: str = "auto"      # stencil compute type for c64 storage: "auto" | "f32" | "f64"
+    eps: float = 0.0
+    safety: float = 0.0
+    dt_decrease: float = 0.0
+    dt_increase: float = 0.0
+
+    def to_c(self) -> L.GpeParams:
+        if self.scheme not in L.SCHEMES:
+            raise ValueError("ERROR: Unrecognised time stepping scheme.")
+        p = L.GpeParams()
+        p.nx, p.ny, p.nz = self.nx, self.ny, self.nz
+        p.scheme = L.SCHEMES[self.scheme]
+        p.eqn, p.bcs, p.order = self.eqn_to_solve, self.bcs, self.order
+        p.real_time = 1 if self.real_time else 0
+        p.storage = {"c128": L.GPE_C128, "c64": L.GPE_C64}[self.storage]
+        p.compute = {"auto": L.GPE_COMPUTE_AUTO, "f32": L.GPE_COMPUTE_F32, "f64": L.GPE_COMPUTE_F64}[self.compute]
+        for f in ("xr", "yr", "zr", "tau", "Urhs", "diss_amp", "scal", "g", "mu", "nn", "omx", "omy",
+                  "omz", "gamma", "eps", "safety", "dt_decrease", "dt_increase"):
+            setattr(p, f, float(getattr(self, f)))
+        return p
+
+    def replace(self, **kw) -> "RunParams":
+        d = {f.name: getattr(self, f.name) for f in fields(self)}
+        d.update(kw)
+        return RunParams(**d)
+
+
+def _check(lib, h, rc: int) -> None:
+    if rc != L.GPE_OK:
+        msg = lib.gpe_last_error(h)
+        raise L.GpeError(rc, msg.decode() if msg else "")
+
+
+class Solver:
+    """One device-resident solve."""
+
+    def __init__(self, params: RunParams):
+        self.lib = L.load()
+        self.params = params
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        rc = self.lib.gpe_create(C.byref(self._cp), C.byref(h))
+        _check(self.lib, None, rc)
+        self.h = h
+        # src/gpe.f90:78-82
+        self.t = 0.0
+        self.im_t = 0.0
+        self.dt = complex(params.tau, 0.0) if params.real_time else complex(0.0, -params.tau)
+        self.p = 0
+        self.last = L.GpeStepInfo()
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.gpe_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state --------------------------------------------------------------
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        return (self.params.nz, self.params.ny, self.params.nx)
+
+    def set_state(self, psi: np.ndarray) -> None:
+        psi = np.asarray(psi)
+        if psi.shape != self.shape:
+            raise ValueError(f"psi must have shape (nz, ny, nx) = {self.shape}")
+        if psi.dtype == np.complex64:
+            arr, dt = np.ascontiguousarray(psi), L.GPE_C64
+        else:
+            arr, dt = np.ascontiguousarray(psi, dtype=np.complex128), L.GPE_C128
+        _check(self.lib, self.h, self.lib.gpe_set_state(self.h, arr.ctypes.data, dt))
+
+    def get_state(self, dtype=np.complex128, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape, dtype=dtype)
+        code = L.GPE_C64 if out.dtype == np.complex64 else L.GPE_C128
+        _check(self.lib, self.h, self.lib.gpe_get_state(self.h, out.ctypes.data, code))
+        return out
+
+    # -- stepping -----------------------------------------------------------
+    def solver(self, nsteps: int = 1, want_norm: bool = False, want_energy: bool = False,
+               wait: bool = True) -> L.GpeStepInfo:
+        """nsteps calls of the reference's solver() with its time update."""
+        io = L.GpeStepInfo()
+        io.t, io.im_t = self.t, self.im_t
+        io.dt_re, io.dt_im = self.dt.real, self.dt.imag
+        io.p = self.p
+        io.want_norm = 1 if want_norm else 0
+        io.want_energy = 1 if want_energy else 0
+        fn = self.lib.gpe_step if wait else self.lib.gpe_step_async
+        _check(self.lib, self.h, fn(self.h, int(nsteps), C.byref(io)))
+        self.t, self.im_t = io.t, io.im_t
+        self.dt = complex(io.dt_re, io.dt_im)
+        self.p = io.p
+        self.last = io
+        return io
+
+    step = solver
+
+    def sync(self) -> None:
+        _check(self.lib, self.h, self.lib.gpe_sync(self.h))
+
+    # -- diagnostics --------------------------------------------------------
+    def get_norm(self) -> float:
+        v = C.c_double()
+        _check(self.lib, self.h, self.lib.gpe_norm(self.h, C.byref(v)))
+        return v.value
+
+    def energy(self) -> float:
+        v = C.c_double()
+        _check(self.lib, self.h, self.lib.gpe_energy(self.h, C.byref(v)))
+        return v.value
+
+    def renormalise(self, norm: float) -> None:
+        _check(self.lib, self.h, self.lib.gpe_renormalise(self.h, float(norm)))
+
+    def grid(self):
+        p = self.params
+        x, y, z = np.empty(p.nx), np.empty(p.ny), np.empty(p.nz)
+        d = np.empty(3)
+        self.lib.gpe_get_grid(self.h, x.ctypes.data, y.ctypes.data, z.ctypes.data, d.ctypes.data)
+        return x, y, z, d
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self.lib.gpe_get_stream(self.h, C.byref(s))
+        return s.value or 0
+
+
+def state_bytes(params: RunParams) -> int:
+    lib = L.load()
+    cp = params.to_c()
+    return int(lib.gpe_state_bytes(C.byref(cp)))

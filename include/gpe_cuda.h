@@ -1,0 +1,179 @@
+/*
+ * gpe_cuda.h -- C ABI of the B200 (sm_100a) Gross-Pitaevskii time-stepper.
+ *
+ * This is the drop-in boundary for the reference's (anthonyyoud/gpe) time
+ * stepping path.  In the reference the path is reached through Fortran module
+ * procedures that read module globals (src/parameters.f90:24-129); here the
+ * same quantities travel in a POD struct and the state lives on the GPU
+ * inside an opaque handle.  Every entry point below names the reference
+ * interface it replaces.
+ *
+ * Conventions
+ *   - Return 0 (GPE_OK) on success, a negative GPE_ERR_* on failure.  The
+ *     reference has no return codes: a host maps any non-zero value onto its
+ *     emergency_stop(gpe_last_error(h)) (src/error.f90:24-46), which keeps the
+ *     ERROR / RUNNING file semantics unchanged.
+ *   - Host arrays are the reference's interior arrays psi(0:nx-1,0:ny-1,
+ *     0:nz-1), Fortran column-major (x fastest), complex (re, im) pairs:
+ *     GPE_C128 = complex(8) / double[2], GPE_C64 = complex(4) / float[2].
+ *   - A handle is not thread-safe; use one host thread per handle.  Distinct
+ *     handles are independent and each owns its own CUDA stream.
+ *   - There is no CPU fallback: without a usable sm_100 GPU, gpe_create
+ *     fails with GPE_ERR_CUDA.
+ */
+#ifndef GPE_CUDA_H
+#define GPE_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPE_OK 0
+#define GPE_ERR_BADARG (-1)
+#define GPE_ERR_CUDA (-2)
+#define GPE_ERR_NONFINITE (-3)
+#define GPE_ERR_TIMEOUT (-4)
+#define GPE_ERR_NOMEM (-5)
+#define GPE_ERR_NOMEM_BUDGET (-6)
+#define GPE_ERR_STATE (-7)
+
+/* time-stepping schemes (src/solve.f90:34-50, run.in `scheme`) */
+#define GPE_EULER 0
+#define GPE_RK2 1
+#define GPE_RK4 2
+#define GPE_RK45 3
+
+/* element types of host arrays and of device storage */
+#define GPE_C128 0
+#define GPE_C64 1
+
+/* Compute type used by the stencil when storage is GPE_C64 */
+#define GPE_COMPUTE_AUTO 0
+#define GPE_COMPUTE_F32 1
+#define GPE_COMPUTE_F64 2
+
+/*
+ * Run parameters.  Field meanings follow the reference's namelists
+ * (src/parameters.f90:40-87) and compile-time grid (src/parameters.in:22-30).
+ * The grid is node-inclusive and symmetric, x_i = -xr + i*2xr/(nx-1)
+ * (src/ic.f90:32-69).
+ */
+typedef struct {
+  int32_t nx, ny, nz;      /* grid points per axis (>= 6)                     */
+  int32_t scheme;          /* GPE_EULER | GPE_RK2 | GPE_RK4 | GPE_RK45        */
+  int32_t eqn;             /* eqn_to_solve 1..4 (src/solve.f90:414-437)       */
+  int32_t bcs;             /* 1 periodic, 2 reflective                        */
+  int32_t order;           /* 2 or 4                                          */
+  int32_t real_time;       /* 1: dt = tau, 0: dt = -i tau (src/gpe.f90:78-82) */
+  int32_t storage;         /* GPE_C128 | GPE_C64 device storage of psi/stages */
+  int32_t compute;         /* GPE_COMPUTE_* (GPE_C64 storage only)            */
+  double xr, yr, zr;       /* half box lengths                                 */
+  double tau;              /* |dt| (run.in tau)                                */
+  double Urhs, diss_amp, scal, g, mu, nn, omx, omy, omz;
+  double gamma;            /* damped eqn 4: rhs = -(i+gamma)(...); 0 = eqn 4  */
+  double eps, safety, dt_decrease, dt_increase; /* RKF45 control; 0 selects the
+                              reference constants 1e-6, 0.9, -0.25, -0.2
+                              (src/parameters.f90:90-93)                      */
+} gpe_params;
+
+/*
+ * In/out record of gpe_step.  t, im_t, dt and p are the reference's globals
+ * (src/parameters.f90:117-129) and are advanced exactly as solver() does.
+ */
+typedef struct {
+  double t, im_t;          /* in/out                                           */
+  double dt_re, dt_im;     /* in/out; RKF45 returns the next trial step        */
+  int64_t p;               /* in/out step index                                */
+  int64_t accepted;        /* out: steps taken in this call                    */
+  int64_t rejected;        /* out: RKF45 rejected attempts in this call        */
+  double errmax;           /* out: last accepted RKF45 error norm              */
+  double norm;             /* out: get_norm of the final state (want_norm)     */
+  double energy;           /* out: energy of the state entering the call       */
+  int32_t want_norm;       /* in                                               */
+  int32_t want_energy;     /* in                                               */
+} gpe_step_info;
+
+typedef struct gpe_handle gpe_handle;
+
+/* Replaces the set-up of src/gpe.f90:59-88 (allocate psi%old/psi%new, dt,
+ * get_grid).  Allocates all device state for one solve. */
+int gpe_create(const gpe_params* p, gpe_handle** out);
+
+/* Frees the handle's device memory and stream (src/gpe.f90:296-304). */
+void gpe_destroy(gpe_handle* h);
+
+/* Message for the last failure on this handle (h may be NULL: the last
+ * failure of gpe_create on this thread).  Feeds emergency_stop. */
+const char* gpe_last_error(const gpe_handle* h);
+
+/* Copy the host interior array in / out (replaces psi%new assignment from
+ * ics(), src/gpe.f90:107, and the reads of psi%new by io.f90's writers).
+ * dtype is GPE_C128 or GPE_C64; synchronous. */
+int gpe_set_state(gpe_handle* h, const void* psi, int32_t dtype);
+int gpe_get_state(gpe_handle* h, void* psi, int32_t dtype);
+
+/* Same as above with a device pointer to a contiguous interior array. */
+int gpe_set_state_device(gpe_handle* h, const void* psi_dev, int32_t dtype);
+int gpe_get_state_device(gpe_handle* h, void* psi_dev, int32_t dtype);
+
+/* nsteps x (solver(psi%old, psi%new) + its time update), src/solve.f90:25-53
+ * called from src/gpe.f90:230, including the halo exchange of
+ * src/gpe.f90:173-176 (replaced by in-kernel boundary conditions).
+ * RKF45 follows rkqs (src/solve.f90:158-244) including its quirks.
+ * Returns after the device work completes. */
+int gpe_step(gpe_handle* h, int64_t nsteps, gpe_step_info* io);
+
+/* Enqueue nsteps fixed-step steps (Euler/RK2/RK4) on the handle's stream
+ * without waiting; io's clock is advanced on return.  gpe_sync waits. */
+int gpe_step_async(gpe_handle* h, int64_t nsteps, gpe_step_info* io);
+int gpe_sync(gpe_handle* h);
+
+/* get_norm (src/variables.f90:554-576) of the current state. */
+int gpe_norm(gpe_handle* h, double* norm);
+/* energy (src/variables.f90:580-604), un-normalised: io.f90:202 divides the
+ * value by nx*ny*nz before writing energy.dat. */
+int gpe_energy(gpe_handle* h, double* energy);
+/* renormalise (src/variables.f90:715-726): psi = sqrt(nn)*psi/sqrt(norm). */
+int gpe_renormalise(gpe_handle* h, double norm);
+
+/* get_grid results (src/ic.f90:32-69): x[nx], y[ny], z[nz], dxyz[3];
+ * any pointer may be NULL. */
+int gpe_get_grid(const gpe_handle* h, double* x, double* y, double* z, double* dxyz);
+
+/* The CUDA stream (cudaStream_t) all of the handle's work runs on. */
+int gpe_get_stream(const gpe_handle* h, void** stream);
+
+/* Stage-kernel kinds reported by gpe_profile_get (one fused kernel each). */
+#define GPE_KIND_EULER 0
+#define GPE_KIND_RK2_1 1
+#define GPE_KIND_RK2_2 2
+#define GPE_KIND_RK4_1 3
+#define GPE_KIND_RK4_23 4
+#define GPE_KIND_RK4_4 5
+#define GPE_KIND_CK_1 6
+#define GPE_KIND_CK_6 11
+#define GPE_KIND_ENERGY 12
+#define GPE_NUM_KINDS 13
+
+/* Instrumentation (no reference counterpart; the reference has no tracing
+ * beyond timestep.dat, src/solve.f90:234-241): with enable = 1, every stage
+ * kernel launch is bracketed by CUDA events on the handle's stream and its
+ * device time accumulated per kind; enable resets the totals. */
+int gpe_profile(gpe_handle* h, int32_t enable);
+/* Total device ms and launch count of one kind since gpe_profile(h, 1), and
+ * the kind's algorithmic HBM bytes per grid site per launch (one read of
+ * each input field, one write of each output field). */
+int gpe_profile_get(gpe_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes_per_site);
+
+/* Bytes of device memory a solve with these parameters allocates. */
+int64_t gpe_state_bytes(const gpe_params* p);
+
+/* Library build/version string. */
+const char* gpe_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPE_CUDA_H */

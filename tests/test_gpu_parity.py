@@ -1,0 +1,211 @@
+"""Parity of the sm_100a stepper (through the C ABI) with the CPU oracle.
+
+Tolerances: FP64 storage <= 1e-12 relative L2 (the target the reference's
+plain FP64 method must meet); FP32 storage <= 1e-5 relative L2 and 1e-7
+relative norm drift against the FP64 oracle where stated.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from gpe_b200 import _lib as L
+from gpe_b200 import ic
+from gpe_b200.solver import RunParams, Solver
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def run_both(rp, psi0, steps, **kw):
+    o = Oracle(rp)
+    ref = o.run(psi0, steps)
+    s = Solver(rp)
+    s.set_state(psi0)
+    info = s.solver(steps, **kw)
+    out = s.get_state()
+    return o, ref, s, out, info
+
+
+def c1_params(**kw):
+    # 64^3 ring, reflective, 2nd order, RK4 dt = 0.01, V = 0, mu = 1 (g = 1);
+    # node-inclusive grid with dx = 0.5 (x_i = -15.75 + 0.5 i)
+    base = dict(nx=64, ny=64, nz=64, xr=15.75, yr=15.75, zr=15.75, tau=0.01, scheme="rk4",
+                eqn_to_solve=4, bcs=2, order=2, g=1.0, mu=1.0)
+    base.update(kw)
+    return RunParams(**base)
+
+
+def test_c1_ring_rk4_1000_steps(gpu):
+    rp = c1_params()
+    psi0 = ic.vortex_ring(rp, "xy", r0=4.0)
+    o, ref, s, out, info = run_both(rp, psi0, 1000, want_norm=True)
+    assert rel_l2(out, ref) <= TOL64
+    assert info.norm == pytest.approx(o.get_norm(ref), rel=TOL64)
+    assert s.energy() == pytest.approx(o.energy(ref), rel=TOL64)
+    assert s.t == o.clock.t and s.im_t == o.clock.im_t and s.p == 1000
+
+
+def test_c1_eqn1_second_parity_case(gpu):
+    rp = c1_params(eqn_to_solve=1)
+    psi0 = ic.vortex_ring(rp, "xy", r0=4.0)
+    o, ref, s, out, info = run_both(rp, psi0, 200)
+    assert rel_l2(out, ref) <= TOL64
+
+
+def golden_cases():
+    from tests.golden.make_golden import CASES
+    return [c[0] for c in CASES]
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_fixtures(gpu, name):
+    from pathlib import Path
+
+    from tests.golden.make_golden import CASES, SHAPE
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "oracle_small.npz")
+    kw = dict(next(c[1] for c in CASES if c[0] == name))
+    rp = RunParams(**SHAPE, **kw)
+    s = Solver(rp)
+    s.set_state(z[f"{name}/psi0"])
+    info = s.solver(int(z[f"{name}/steps"]), want_norm=True)
+    out = s.get_state()
+    assert rel_l2(out, z[f"{name}/psi"]) <= TOL64
+    assert info.norm == pytest.approx(float(z[f"{name}/norm"]), rel=TOL64)
+    assert s.energy() == pytest.approx(float(z[f"{name}/energy"]), rel=TOL64)
+    clk = z[f"{name}/clock"]
+    assert s.t == pytest.approx(clk[0], rel=1e-12, abs=1e-300)
+    assert s.im_t == pytest.approx(clk[1], rel=1e-12, abs=1e-300)
+    if kw.get("scheme") == "rk45":
+        assert (s.dt.real, s.dt.imag) == pytest.approx((clk[2], clk[3]), rel=1e-12)
+
+
+SIZES = [(17, 13, 11), (33, 20, 9), (40, 7, 12)]
+
+
+@pytest.mark.parametrize("shape", SIZES)
+@pytest.mark.parametrize("eqn", [1, 2, 3, 4])
+@pytest.mark.parametrize("bcs", [1, 2])
+@pytest.mark.parametrize("order", [2, 4])
+def test_matrix_rk4(gpu, shape, eqn, bcs, order):
+    nx, ny, nz = shape
+    rp = RunParams(nx=nx, ny=ny, nz=nz, xr=4.0, yr=3.0, zr=2.0, tau=0.003, scheme="rk4", eqn_to_solve=eqn,
+                   bcs=bcs, order=order, g=1.3, mu=0.7, omx=0.2, omy=0.3, omz=0.1,
+                   Urhs=0.2 if eqn != 4 else 0.0, diss_amp=0.1 if eqn in (1, 3) else 0.0)
+    rng = np.random.default_rng(nx * 100 + eqn * 10 + bcs + order)
+    psi0 = (rng.standard_normal((nz, ny, nx)) + 1j * rng.standard_normal((nz, ny, nx))) * 0.3 + 1.0
+    o, ref, s, out, info = run_both(rp, psi0, 4)
+    assert rel_l2(out, ref) <= TOL64
+
+
+@pytest.mark.parametrize("scheme", ["euler", "rk2", "rk4", "rk45"])
+@pytest.mark.parametrize("real_time", [True, False])
+def test_schemes_real_and_imaginary_time(gpu, scheme, real_time):
+    rp = RunParams(nx=24, ny=22, nz=20, xr=5.0, yr=5.0, zr=5.0, tau=0.004, scheme=scheme, eqn_to_solve=4,
+                   bcs=2, order=4, g=1.0, mu=2.0, omx=0.3, omy=0.3, omz=0.2, real_time=real_time)
+    psi0 = ic.fermi(rp) * ic.vortex_line_pade(rp, dir="z")
+    o, ref, s, out, info = run_both(rp, psi0, 8)
+    assert rel_l2(out, ref) <= TOL64
+    assert s.t == pytest.approx(o.clock.t, rel=1e-12, abs=1e-300)
+    assert s.im_t == pytest.approx(o.clock.im_t, rel=1e-12, abs=1e-300)
+
+
+def test_rk45_step_control_sequence(gpu):
+    # large initial tau forces rejections; dt sequence must follow the oracle
+    rp = RunParams(nx=24, ny=20, nz=28, xr=4.0, yr=4.0, zr=5.0, tau=0.2, scheme="rk45", eqn_to_solve=4,
+                   bcs=2, order=4, g=1.0, mu=10.0, omx=0.05, omy=0.05, omz=0.025, gamma=0.05)
+    psi0 = ic.fermi(rp) * ic.vortex_line_pade(rp, dir="z")
+    o = Oracle(rp)
+    s = Solver(rp)
+    s.set_state(psi0)
+    psi = psi0
+    for _ in range(6):
+        psi = o.run(psi, 1)
+        s.solver(1)
+        assert s.dt.real == pytest.approx(o.clock.dt_re, rel=1e-10)
+        assert s.t == pytest.approx(o.clock.t, rel=1e-12)
+    assert rel_l2(s.get_state(), psi) <= 1e-11
+    assert o.clock.rejected >= 1
+
+
+def test_norm_energy_renormalise(gpu):
+    rp = RunParams(nx=30, ny=26, nz=22, xr=5.0, yr=4.0, zr=3.0, bcs=1, order=4, nn=3.0)
+    rng = np.random.default_rng(3)
+    psi0 = rng.standard_normal((22, 26, 30)) + 1j * rng.standard_normal((22, 26, 30))
+    o = Oracle(rp)
+    s = Solver(rp)
+    s.set_state(psi0)
+    n = s.get_norm()
+    assert n == pytest.approx(o.get_norm(psi0), rel=1e-13)
+    assert s.energy() == pytest.approx(o.energy(psi0), rel=1e-12)
+    s.renormalise(n)
+    assert rel_l2(s.get_state(), o.renormalise(psi0, n)) <= 1e-15
+    assert s.get_norm() == pytest.approx(3.0, rel=1e-13)
+
+
+def test_fused_energy_equals_standalone(gpu):
+    rp = c1_params(nx=40, ny=36, nz=32)
+    psi0 = ic.vortex_ring(rp, "xy", r0=4.0)
+    s = Solver(rp)
+    s.set_state(psi0)
+    e0 = s.energy()
+    info = s.solver(3, want_energy=True, want_norm=True)
+    assert info.energy == pytest.approx(e0, rel=1e-13)
+    assert info.norm == pytest.approx(s.get_norm(), rel=1e-13)
+
+
+def test_state_roundtrip_both_dtypes(gpu):
+    rp = RunParams(nx=19, ny=17, nz=15, storage="c128")
+    rng = np.random.default_rng(11)
+    psi = rng.standard_normal((15, 17, 19)) + 1j * rng.standard_normal((15, 17, 19))
+    s = Solver(rp)
+    s.set_state(psi)
+    np.testing.assert_array_equal(s.get_state(), psi)
+    s.set_state(psi.astype(np.complex64))
+    np.testing.assert_array_equal(s.get_state(np.complex64), psi.astype(np.complex64))
+
+
+def test_nonfinite_is_reported(gpu):
+    rp = RunParams(nx=16, ny=16, nz=16)
+    psi = np.ones((16, 16, 16), np.complex128)
+    psi[3, 4, 5] = np.nan
+    s = Solver(rp)
+    s.set_state(psi)
+    with pytest.raises(L.GpeError) as e:
+        s.solver(1, want_norm=True)
+    assert e.value.code == L.GPE_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("compute", ["f32", "f64"])
+def test_fp32_storage_vs_fp64_oracle(gpu, compute):
+    rp = c1_params(nx=48, ny=48, nz=48, xr=11.75, yr=11.75, zr=11.75, bcs=1, order=4, eqn_to_solve=2,
+                   tau=0.005)
+    psi0 = ic.random_phase(rp, seed=5, kc=1.5)
+    o = Oracle(rp)
+    ref = o.run(psi0, 200)
+    s = Solver(rp.replace(storage="c64", compute=compute))
+    s.set_state(psi0)
+    info = s.solver(200, want_norm=True)
+    out = s.get_state()
+    err = rel_l2(out, ref)
+    drift = abs(info.norm - o.get_norm(ref)) / o.get_norm(ref)
+    print(f"fp32 storage ({compute} compute): rel_l2={err:.3e} norm drift={drift:.3e}")
+    assert err <= 1e-5
+    assert drift <= 1e-7
+
+
+@pytest.mark.slow
+def test_c2_256_cubed_periodic_o4(gpu):
+    rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
+                   eqn_to_solve=2, bcs=1, order=4)
+    psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
+    o, ref, s, out, info = run_both(rp, psi0, 4, want_norm=True)
+    assert rel_l2(out, ref) <= TOL64
+    assert info.norm == pytest.approx(o.get_norm(ref), rel=TOL64)
