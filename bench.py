@@ -193,6 +193,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="device-resident leg only (tuning sweeps)")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="profiling target: set up the workload and run 2 RK4 steps, nothing else")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -200,15 +203,10 @@ def main() -> int:
 
     import torch
 
+    from gpe_b200 import dist
+
     torch.cuda.set_device(local)
-    pg = None
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    pg = dist.init(backend="nccl", timeout_s=120)
 
     from gpe_b200 import _lib as L
     from gpe_b200 import ic
@@ -220,19 +218,17 @@ def main() -> int:
     s = Solver(rp)
     s.set_state(psi0)
     stream = torch.cuda.ExternalStream(s.stream())
+    if args.ncu_case:
+        s.solver(2)
+        s.close()
+        return 0
 
     def barrier():
         torch.cuda.synchronize()
-        if pg is not None:
-            pg.barrier()
+        dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = dist.max_over_ranks
 
     # ---- device-resident throughput -------------------------------------
     for _ in range(args.warmup):
@@ -278,6 +274,13 @@ def main() -> int:
                 "all_stage_kernels_gbs": step_bytes / (step_ms * 1e-3) / 1e9,
                 "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()}}
 
+    if args.quick:
+        s.close()
+        if rank == 0:
+            print(json.dumps({"value": value, "unit": UNIT, "ms_per_step": ms / args.steps,
+                              "zc": os.environ.get("GPE_ZC"), "roofline": roofline}), flush=True)
+        return 0
+
     # ---- end to end through the C ABI with host buffers ------------------
     host_in = torch.empty((rp.nz, rp.ny, rp.nx), dtype=torch.complex128, pin_memory=True)
     host_in.numpy()[...] = psi0
@@ -314,8 +317,7 @@ def main() -> int:
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg is not None:
-        pg.barrier()
-        pg.destroy_process_group()
+        dist.finalize()
     return 0
 
 

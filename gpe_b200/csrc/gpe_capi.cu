@@ -4,6 +4,8 @@
 // stream, reduction buffers.  gpe_step() enqueues one fused stage kernel per
 // Runge-Kutta stage; the time bookkeeping follows the reference's solver()
 // routines (src/solve.f90:57-244) on the host, in FP64.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,11 +19,18 @@
 #include "../../include/gpe_cuda.h"
 #include "gpe_aux.cuh"
 #include "gpe_device.cuh"
+#include "gpe_stage_tma.cuh"
 
 namespace gpe {
 cudaError_t launch_stage_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
 cudaError_t launch_stage_f32(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
 cudaError_t launch_stage_f32x(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
+cudaError_t launch_stage_tma_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
+                                 const StageArgs& a);
+cudaError_t launch_stage_tma_f32(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
+                                 const StageArgs& a);
+cudaError_t launch_stage_tma_f32x(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
+                                  const StageArgs& a);
 }  // namespace gpe
 
 using namespace gpe;
@@ -75,6 +84,10 @@ struct gpe_handle {
   size_t ev_used = 0;              // pairs in flight
   double prof_ms[K_NUM] = {0};
   long long prof_n[K_NUM] = {0};
+  // kernel variant: true = TMA plane pipeline (k_stage_tma), false = k_stage
+  bool use_tma = true;
+  std::vector<CUtensorMap> map_halo, map_pw;  // per field
+  int* status = nullptr;                      // device status word
 };
 
 namespace {
@@ -144,11 +157,80 @@ int choose_zc(const Geom& g) {
   return (int)std::min<long long>(zc, g.nz);
 }
 
-cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a) {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// Tensor maps of one ghost-padded field: rank 3 over (2*px scalars, ny+4
+// rows, nz+4 planes); box = halo'd stencil tile or plain point-wise tile.
+bool encode_field_maps(gpe_handle* h, void* base, CUtensorMap* halo, CUtensorMap* pw) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const Geom& g = h->g;
+  const CUtensorMapDataType dt = h->esz == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)(2 * g.px), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
+  const cuuint64_t strides[2] = {(cuuint64_t)(g.px * h->esz), (cuuint64_t)(g.pz * h->esz)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint32_t box_h[3] = {(cuuint32_t)(2 * tma_stencil_w()), (cuuint32_t)tma_stencil_h(8, h->R), 1};
+  const cuuint32_t box_p[3] = {(cuuint32_t)(2 * TMA_TX), 8, 1};
+  if (enc(halo, dt, 3, base, dims, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  if (enc(pw, dt, 3, base, dims, strides, box_p, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  return true;
+}
+
+int field_of(const gpe_handle* h, const void* p) {
+  for (size_t f = 0; f < h->fields.size(); ++f)
+    if (h->fields[f] == p) return (int)f;
+  return -1;
+}
+
+cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a_in) {
+  StageArgs a = a_in;
+  a.status = h->status;
+  if (!h->use_tma) {
+    switch (h->cmode) {
+      case CM_F64: return launch_stage_f64(kind, h->R, 8, h->grid, h->st, a);
+      case CM_F32: return launch_stage_f32(kind, h->R, 8, h->grid, h->st, a);
+      default: return launch_stage_f32x(kind, h->R, 8, h->grid, h->st, a);
+    }
+  }
+  TmaMaps m;
+  memset(&m, 0, sizeof(m));
+  const int fin = field_of(h, a.in);
+  if (fin < 0) return cudaErrorInvalidValue;
+  m.in = h->map_halo[fin];
+  // point-wise inputs in the order of StageTraits: psi, acc, K...
+  const bool has_psi = (kind == K_RK2_2 || kind == K_RK4_2 || (kind >= K_CK_2 && kind <= K_CK_6));
+  const bool has_acc = (kind == K_RK4_2 || kind == K_RK4_4);
+  const int nk = (kind >= K_CK_2 && kind <= K_CK_5) ? (kind - K_CK_1) : (kind == K_CK_6 ? 4 : 0);
+  int q = 0;
+  const void* pws[7];
+  if (has_psi) pws[q++] = a.psi;
+  if (has_acc) pws[q++] = a.acc;
+  for (int t = 0; t < nk; ++t) pws[q++] = a.kin[t];
+  for (int t = 0; t < q; ++t) {
+    const int f = field_of(h, pws[t]);
+    if (f < 0) return cudaErrorInvalidValue;
+    m.pw[t] = h->map_pw[f];
+  }
   switch (h->cmode) {
-    case CM_F64: return launch_stage_f64(kind, h->R, 8, h->grid, h->st, a);
-    case CM_F32: return launch_stage_f32(kind, h->R, 8, h->grid, h->st, a);
-    default: return launch_stage_f32x(kind, h->R, 8, h->grid, h->st, a);
+    case CM_F64: return launch_stage_tma_f64(kind, h->R, 8, h->grid, h->st, m, a);
+    case CM_F32: return launch_stage_tma_f32(kind, h->R, 8, h->grid, h->st, m, a);
+    default: return launch_stage_tma_f32x(kind, h->R, 8, h->grid, h->st, m, a);
   }
 }
 
@@ -294,11 +376,23 @@ int finalize_into(gpe_handle* h, const double* part, int slot) {
   return GPE_OK;
 }
 
+// A stage kernel whose bounded mbarrier wait expired leaves a non-zero
+// status word; report it as GPE_ERR_TIMEOUT (and clear it).
+int check_status(gpe_handle* h) {
+  int st = 0;
+  CU(h, cudaMemcpy(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    CU(h, cudaMemset(h->status, 0, sizeof(int)));
+    return fail(h, GPE_ERR_TIMEOUT, "a stage kernel's bounded wait for its TMA copies expired");
+  }
+  return GPE_OK;
+}
+
 int fetch_results(gpe_handle* h) {
   CU(h, cudaMemcpyAsync(h->hres, h->dres, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   if (h->prof) prof_resolve(h);
-  return GPE_OK;
+  return check_status(h);
 }
 
 double rk_param(double v, double def) { return v != 0.0 ? v : def; }
@@ -579,6 +673,22 @@ int gpe_create(const gpe_params* p, gpe_handle** out) {
     }
     cudaMemsetAsync(h->fields[f], 0, (size_t)h->nelem * h->esz, h->st);
   }
+  if (const char* e = getenv("GPE_KERNEL")) h->use_tma = strcmp(e, "ldg") != 0;
+  if (h->use_tma) {
+    h->map_halo.resize(nf);
+    h->map_pw.resize(nf);
+    for (int f = 0; f < nf; ++f)
+      if (!encode_field_maps(h, h->fields[f], &h->map_halo[f], &h->map_pw[f])) {
+        h->err = "cuTensorMapEncodeTiled failed (driver entry point unavailable or bad layout)";
+        return bail(GPE_ERR_CUDA);
+      }
+  }
+  if (cudaMalloc(&h->status, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    h->err = "out of device memory (status word)";
+    return bail(GPE_ERR_NOMEM);
+  }
+  cudaMemsetAsync(h->status, 0, sizeof(int), h->st);
   std::vector<double> tab;
   build_tables(h, tab);
   if (cudaMalloc(&h->tables, tab.size() * sizeof(double)) != cudaSuccess ||
@@ -612,6 +722,7 @@ void gpe_destroy(gpe_handle* h) {
   if (h->dres) cudaFree(h->dres);
   if (h->hres) cudaFreeHost(h->hres);
   if (h->staging) cudaFree(h->staging);
+  if (h->status) cudaFree(h->status);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -704,7 +815,7 @@ int gpe_sync(gpe_handle* h) {
   CU(h, cudaSetDevice(h->dev));
   CU(h, cudaStreamSynchronize(h->st));
   if (h->prof) prof_resolve(h);
-  return GPE_OK;
+  return check_status(h);
 }
 
 int gpe_profile(gpe_handle* h, int32_t enable) {

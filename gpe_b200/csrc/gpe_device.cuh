@@ -77,6 +77,7 @@ struct StageArgs {
   const double *wx, *wy, *wz;   // norm quadrature weights
   const double *cx, *cy, *cz;   // coordinates (sphere)
   double* partials;             // [nblocks][RED_SLOTS]
+  int* status;                  // device status word: non-zero = a bounded wait expired
 };
 
 template <class S>
@@ -267,7 +268,155 @@ __device__ __forceinline__ void block_reduce_store(double v0, double v1, double 
 }
 
 // ---------------------------------------------------------------------------
-// The fused stage kernel.
+// Per-stage data flow (which point-wise fields a stage reads).
+// ---------------------------------------------------------------------------
+template <int KIND>
+struct StageTraits {
+  static constexpr bool HAS_PSI = (KIND == K_RK2_2 || KIND == K_RK4_2 || (KIND >= K_CK_2 && KIND <= K_CK_6));
+  static constexpr bool HAS_ACC = (KIND == K_RK4_2 || KIND == K_RK4_4);
+  // Cash-Karp K inputs: stages 2..5 read K_1..K_{m-1}; stage 6 reads K1, K3,
+  // K4, K5 (K2 only enters with the zero weights c2 = dc2 = 0).
+  static constexpr int NK = (KIND >= K_CK_2 && KIND <= K_CK_5) ? (KIND - K_CK_1) : (KIND == K_CK_6 ? 4 : 0);
+  static constexpr int NPW = (HAS_PSI ? 1 : 0) + (HAS_ACC ? 1 : 0) + NK;  // point-wise input fields
+  static constexpr bool FIRST = (KIND == K_ENERGY || KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 ||
+                                 KIND == K_CK_1);
+};
+
+// stencil neighbourhood of one site
+template <class C>
+struct Nb {
+  cx<C> c0, xm1, xp1, xm2, xp2, ym1, yp1, ym2, yp2, zm1, zp1, zm2, zp2;
+};
+
+// Per-column constants hoisted out of the z loop.
+struct ColumnConsts {
+  double wxy, vxy, sxy;
+  int gx, gy;
+};
+
+__device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i, int j, int R, bool active) {
+  ColumnConsts c;
+  c.wxy = active ? a.wx[i] * a.wy[j] : 0.0;
+  c.vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
+  c.sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
+  c.gx = ghost_pos(i, a.g.nx, R, a.bcs);
+  c.gy = ghost_pos(j, a.g.ny, R, a.bcs);
+  return c;
+}
+
+// Everything a stage does at one interior site (i,j,k) once its stencil
+// neighbourhood and point-wise inputs are in registers: Laplacian, GP
+// right-hand side, the stage combination, the stores (with ghosts) and the
+// fused reductions.  pw[] holds the point-wise inputs in the order
+// psi, acc, K... of StageTraits.
+template <class S, class C, int R, int KIND>
+__device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, const S* pw, int i, int j, int k,
+                                           long long col, const ColumnConsts& cc, double& r_norm, double& r_en,
+                                           double& r_err) {
+  using T = StageTraits<KIND>;
+  const Geom& g = a.g;
+  const cx<C> lxx = d2<C, R>(n.xm2, n.xm1, n.c0, n.xp1, n.xp2, (C)a.ixx);
+  const cx<C> lyy = d2<C, R>(n.ym2, n.ym1, n.c0, n.yp1, n.yp2, (C)a.iyy);
+  const cx<C> lzz = d2<C, R>(n.zm2, n.zm1, n.c0, n.zp1, n.zp2, (C)a.izz);
+  cx<C> lap;
+  lap.r = (lxx.r + lyy.r) + lzz.r;
+  lap.i = (lxx.i + lyy.i) + lzz.i;
+
+  const int gz = ghost_pos(k, g.nz, R, a.bcs);
+  const long long o = (long long)(k + 2) * g.pz + col;
+  const double cr = (double)n.c0.r, ci = (double)n.c0.i;
+
+  if constexpr (T::FIRST) {
+    if (a.want_energy) {
+      // real(-lap * conjg(psi) + 0.5 |psi|^4)   (variables.f90:591-592)
+      const double n2 = cr * cr + ci * ci;
+      r_en += (-(double)lap.r * cr - (double)lap.i * ci) + 0.5 * (n2 * n2);
+    }
+  }
+  if constexpr (KIND != K_ENERGY) {
+    S pv = szero<S>(), av = szero<S>();
+    int q = 0;
+    if constexpr (T::HAS_PSI) pv = pw[q++];
+    if constexpr (T::HAS_ACC) av = pw[q++];
+    const S* kv = pw + q;
+
+    cx<C> dpx{0, 0};
+    if (a.has_urhs) dpx = d1<C, R>(n.xm2, n.xm1, n.xp1, n.xp2, (C)a.ix1);
+    const cx<C> f = gp_rhs<C>(a, n.c0, lap, dpx, cc.vxy, cc.sxy, i, j, k);
+    const cx<double> fd{(double)f.r, (double)f.i};
+    S* out = (S*)a.out;
+
+    if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 || KIND == K_RK4_2 ||
+                  KIND == K_RK4_4) {
+      // out = base + cf0 * f
+      cx<double> base;
+      if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
+      else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
+      else base = cx<double>{cr, ci};
+      const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
+      const S ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
+      store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, ns);
+      if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
+        // acc = (psi | acc) + cf1 * f
+        const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
+        const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
+        ((S*)a.acc)[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
+      }
+      if constexpr (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4) {
+        if (a.want_norm) {
+          const double sr = (double)ns.x, si = (double)ns.y;
+          r_norm += (cc.wxy * a.wz[k]) * (sr * sr + si * si);
+        }
+      }
+    } else {
+      // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
+      const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
+      const S Ks = to_s<S>(Km);
+      const cx<double> Kmd = to_c<double>(Ks);
+      const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
+      if constexpr (KIND != K_CK_6) {
+        ((S*)a.kout)[o] = Ks;
+        double tr = pd.r, ti = pd.i;
+#pragma unroll
+        for (int m = 0; m < T::NK; ++m) {
+          const cx<double> km = to_c<double>(kv[m]);
+          tr = tr + a.b[m] * km.r;
+          ti = ti + a.b[m] * km.i;
+        }
+        tr = tr + a.b[T::NK] * Kmd.r;
+        ti = ti + a.b[T::NK] * Kmd.i;
+        store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<double>{tr, ti}));
+      } else {
+        // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
+        // contribute exact zeros and are skipped.
+        const cx<double> k1 = to_c<double>(kv[0]), k3 = to_c<double>(kv[1]);
+        const cx<double> k4 = to_c<double>(kv[2]), k5 = to_c<double>(kv[3]);
+        const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
+        const double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0;
+        const double DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0, DC6 = C6 - 0.25;
+        const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
+        const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
+        const S ns = to_s<S>(cx<double>{nr, ni});
+        store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, ns);
+        const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
+        const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
+        // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
+        const double fa = hypot(k1.r, k1.i) * a.inv_adt;
+        const double sr = (hypot(pd.r, pd.i) + a.dte_r * fa) + 1e-30;
+        const double si = a.dte_i * fa;
+        const double ratio = hypot(er, ei) / hypot(sr, si);
+        r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
+        if (a.want_norm) {
+          const double qr = (double)ns.x, qi = (double)ns.y;
+          r_norm += (cc.wxy * a.wz[k]) * (qr * qr + qi * qi);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel (load/store-unit version).
 //
 // Block = 32 (x) x TY (y) threads owning an x-y tile and marching over zc
 // planes in z.  Per plane: the centre plane's tile plus a radius-R halo sits
@@ -278,15 +427,12 @@ __device__ __forceinline__ void block_reduce_store(double v0, double v1, double 
 // ---------------------------------------------------------------------------
 template <class S, class C, int R, int KIND, int TY>
 __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
+  using T = StageTraits<KIND>;
   constexpr int TX = 32, NT = TX * TY;
   constexpr int TW = TX + 2 * R, TH = TY + 2 * R;
   constexpr int NH = 2 * R * TX + 2 * R * TY;  // halo points per plane
   constexpr int HPT = (NH + NT - 1) / NT;      // halo points per thread
-  constexpr bool HAS_PSI = (KIND == K_RK2_2 || KIND == K_RK4_2 || (KIND >= K_CK_2 && KIND <= K_CK_6));
-  constexpr bool HAS_ACC = (KIND == K_RK4_2 || KIND == K_RK4_4);
-  // Cash-Karp K inputs: stages 2..5 read K_1..K_{m-1}; stage 6 reads K1, K3,
-  // K4, K5 (K2 only enters with the zero weights c2 = dc2 = 0).
-  constexpr int NK = (KIND >= K_CK_2 && KIND <= K_CK_5) ? (KIND - K_CK_1) : (KIND == K_CK_6 ? 4 : 0);
+  constexpr int NPW = T::NPW > 0 ? T::NPW : 1;
 
   __shared__ S tile[TH * TW];
 
@@ -324,12 +470,17 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
     hsm[h] = (p < NH) ? hy * TW + hx : 0;
     hcol[h] = (long long)(gj + 2) * g.px + g.xoff + gi;
   }
+  const ColumnConsts cc = column_consts(a, i, j, R, active);
 
-  const int gx = ghost_pos(i, g.nx, R, a.bcs);
-  const int gy = ghost_pos(j, g.ny, R, a.bcs);
-  const double wxy = active ? a.wx[i] * a.wy[j] : 0.0;
-  const double vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
-  const double sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
+  // point-wise input pointers in StageTraits order
+  const S* pwp[NPW];
+  {
+    int q = 0;
+    if constexpr (T::HAS_PSI) pwp[q++] = (const S*)a.psi;
+    if constexpr (T::HAS_ACC) pwp[q++] = (const S*)a.acc;
+#pragma unroll
+    for (int m = 0; m < T::NK; ++m) pwp[q++] = (const S*)a.kin[m];
+  }
 
   // z queue and halo of the first plane
   S q[2 * R + 1];
@@ -338,19 +489,12 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
   S hv[HPT];
 #pragma unroll
   for (int h = 0; h < HPT; ++h) hv[h] = hok[h] ? ldro(in + (long long)(kb + 2) * g.pz + hcol[h]) : szero<S>();
-
-  // point-wise inputs of the first plane
-  const S* psi = (const S*)a.psi;
-  S* acc = (S*)a.acc;
-  S pv = szero<S>(), av = szero<S>();
-  S kv[NK > 0 ? NK : 1];
-  if (active) {
-    const long long o = (long long)(kb + 2) * g.pz + col;
-    if constexpr (HAS_PSI) pv = ldro(psi + o);
-    if constexpr (HAS_ACC) av = acc[o];
+  S pv[NPW];
 #pragma unroll
-    for (int m = 0; m < NK; ++m) kv[m] = ldro((const S*)a.kin[m] + o);
-  }
+  for (int m = 0; m < T::NPW; ++m)
+    pv[m] = active ? (T::HAS_ACC && m == (T::HAS_PSI ? 1 : 0) ? pwp[m][(long long)(kb + 2) * g.pz + col]
+                                                              : ldro(pwp[m] + (long long)(kb + 2) * g.pz + col))
+                   : szero<S>();
 
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
 
@@ -359,19 +503,16 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
     // prefetch the next iteration's loads
     S qn = szero<S>();
     S hn[HPT];
-    S pn = szero<S>(), an = szero<S>();
-    S kn[NK > 0 ? NK : 1];
+    S pn[NPW];
     if (more) {
       if (ldok) qn = ldro(in + (long long)(k + R + 3) * g.pz + col);
 #pragma unroll
       for (int h = 0; h < HPT; ++h) hn[h] = hok[h] ? ldro(in + (long long)(k + 3) * g.pz + hcol[h]) : szero<S>();
-      if (active) {
-        const long long o = (long long)(k + 3) * g.pz + col;
-        if constexpr (HAS_PSI) pn = ldro(psi + o);
-        if constexpr (HAS_ACC) an = acc[o];
 #pragma unroll
-        for (int m = 0; m < NK; ++m) kn[m] = ldro((const S*)a.kin[m] + o);
-      }
+      for (int m = 0; m < T::NPW; ++m)
+        pn[m] = active ? (T::HAS_ACC && m == (T::HAS_PSI ? 1 : 0) ? pwp[m][(long long)(k + 3) * g.pz + col]
+                                                                  : ldro(pwp[m] + (long long)(k + 3) * g.pz + col))
+                       : szero<S>();
     }
 
     __syncthreads();
@@ -383,113 +524,25 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
 
     if (active) {
       const int ts = (ty + R) * TW + tx + R;
-      const cx<C> c0 = to_c<C>(q[R]);
-      cx<C> xm2{0, 0}, xp2{0, 0}, ym2{0, 0}, yp2{0, 0}, zm2{0, 0}, zp2{0, 0};
-      const cx<C> xm1 = to_c<C>(tile[ts - 1]), xp1 = to_c<C>(tile[ts + 1]);
-      const cx<C> ym1 = to_c<C>(tile[ts - TW]), yp1 = to_c<C>(tile[ts + TW]);
-      const cx<C> zm1 = to_c<C>(q[R - 1]), zp1 = to_c<C>(q[R + 1]);
+      Nb<C> n;
+      n.c0 = to_c<C>(q[R]);
+      n.xm1 = to_c<C>(tile[ts - 1]);
+      n.xp1 = to_c<C>(tile[ts + 1]);
+      n.ym1 = to_c<C>(tile[ts - TW]);
+      n.yp1 = to_c<C>(tile[ts + TW]);
+      n.zm1 = to_c<C>(q[R - 1]);
+      n.zp1 = to_c<C>(q[R + 1]);
       if constexpr (R == 2) {
-        xm2 = to_c<C>(tile[ts - 2]);
-        xp2 = to_c<C>(tile[ts + 2]);
-        ym2 = to_c<C>(tile[ts - 2 * TW]);
-        yp2 = to_c<C>(tile[ts + 2 * TW]);
-        zm2 = to_c<C>(q[0]);
-        zp2 = to_c<C>(q[4]);
+        n.xm2 = to_c<C>(tile[ts - 2]);
+        n.xp2 = to_c<C>(tile[ts + 2]);
+        n.ym2 = to_c<C>(tile[ts - 2 * TW]);
+        n.yp2 = to_c<C>(tile[ts + 2 * TW]);
+        n.zm2 = to_c<C>(q[0]);
+        n.zp2 = to_c<C>(q[4]);
+      } else {
+        n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
       }
-      const cx<C> lxx = d2<C, R>(xm2, xm1, c0, xp1, xp2, (C)a.ixx);
-      const cx<C> lyy = d2<C, R>(ym2, ym1, c0, yp1, yp2, (C)a.iyy);
-      const cx<C> lzz = d2<C, R>(zm2, zm1, c0, zp1, zp2, (C)a.izz);
-      cx<C> lap;
-      lap.r = (lxx.r + lyy.r) + lzz.r;
-      lap.i = (lxx.i + lyy.i) + lzz.i;
-
-      const int gz = ghost_pos(k, g.nz, R, a.bcs);
-      const long long o = (long long)(k + 2) * g.pz + col;
-      const double cr = (double)c0.r, ci = (double)c0.i;
-
-      if constexpr (KIND == K_ENERGY || KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_CK_1) {
-        if (a.want_energy) {
-          // real(-lap * conjg(psi) + 0.5 |psi|^4)   (variables.f90:591-592)
-          const double n2 = cr * cr + ci * ci;
-          r_en += (-(double)lap.r * cr - (double)lap.i * ci) + 0.5 * (n2 * n2);
-        }
-      }
-
-      if constexpr (KIND != K_ENERGY) {
-        cx<C> dpx{0, 0};
-        if (a.has_urhs) dpx = d1<C, R>(xm2, xm1, xp1, xp2, (C)a.ix1);
-        const cx<C> f = gp_rhs<C>(a, c0, lap, dpx, vxy, sxy, i, j, k);
-        const cx<double> fd{(double)f.r, (double)f.i};
-        S* out = (S*)a.out;
-
-        if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 ||
-                      KIND == K_RK4_2 || KIND == K_RK4_4) {
-          // out = base + cf0 * f
-          cx<double> base;
-          if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
-          else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
-          else base = cx<double>{cr, ci};
-          const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
-          const cx<double> nv{base.r + t0.r, base.i + t0.i};
-          const S ns = to_s<S>(nv);
-          store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, ns);
-          if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
-            // acc = (psi | acc) + cf1 * f
-            const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
-            const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
-            acc[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
-          }
-          if constexpr (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4) {
-            if (a.want_norm) {
-              const double sr = (double)ns.x, si = (double)ns.y;
-              r_norm += (wxy * a.wz[k]) * (sr * sr + si * si);
-            }
-          }
-        } else {
-          // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
-          const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
-          const S Ks = to_s<S>(Km);
-          const cx<double> Kmd = to_c<double>(Ks);
-          const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
-          if constexpr (KIND != K_CK_6) {
-            ((S*)a.kout)[o] = Ks;
-            double tr = pd.r, ti = pd.i;
-#pragma unroll
-            for (int m = 0; m < NK; ++m) {
-              const cx<double> km = to_c<double>(kv[m]);
-              tr = tr + a.b[m] * km.r;
-              ti = ti + a.b[m] * km.i;
-            }
-            tr = tr + a.b[NK] * Kmd.r;
-            ti = ti + a.b[NK] * Kmd.i;
-            store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, to_s<S>(cx<double>{tr, ti}));
-          } else {
-            // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
-            // contribute exact zeros and are skipped.
-            const cx<double> k1 = to_c<double>(kv[0]), k3 = to_c<double>(kv[1]);
-            const cx<double> k4 = to_c<double>(kv[2]), k5 = to_c<double>(kv[3]);
-            const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
-            const double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0;
-            const double DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0, DC6 = C6 - 0.25;
-            const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
-            const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
-            const S ns = to_s<S>(cx<double>{nr, ni});
-            store_with_ghosts(out, g, col, i, j, k, gx, gy, gz, ns);
-            const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
-            const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
-            // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
-            const double fa = hypot(k1.r, k1.i) * a.inv_adt;
-            const double sr = (hypot(pd.r, pd.i) + a.dte_r * fa) + 1e-30;
-            const double si = a.dte_i * fa;
-            const double ratio = hypot(er, ei) / hypot(sr, si);
-            r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
-            if (a.want_norm) {
-              const double qr = (double)ns.x, qi = (double)ns.y;
-              r_norm += (wxy * a.wz[k]) * (qr * qr + qi * qi);
-            }
-          }
-        }
-      }
+      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, col, cc, r_norm, r_en, r_err);
     }
 
     // rotate the queue
@@ -498,10 +551,8 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
     q[2 * R] = qn;
 #pragma unroll
     for (int h = 0; h < HPT; ++h) hv[h] = hn[h];
-    pv = pn;
-    av = an;
 #pragma unroll
-    for (int m = 0; m < NK; ++m) kv[m] = kn[m];
+    for (int m = 0; m < T::NPW; ++m) pv[m] = pn[m];
   }
 
   if (a.partials) block_reduce_store<NT>(r_norm, r_en, r_err, a.partials);
