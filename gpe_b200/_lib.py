@@ -73,6 +73,8 @@ _PROTOS = {
     "gpe_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "gpe_profile_get": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                   C.POINTER(C.c_double)]),
+    "gpe_norm_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                   C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
 }
 
 KIND_NAMES = ["euler", "rk2_1", "rk2_2", "rk4_1", "rk4_23", "rk4_4", "ck_1", "ck_2", "ck_3", "ck_4", "ck_5",

@@ -170,6 +170,34 @@ int gpe_profile_get(gpe_handle* h, int32_t kind, double* total_ms, int64_t* laun
 /* Bytes of device memory a solve with these parameters allocates. */
 int64_t gpe_state_bytes(const gpe_params* p);
 
+/*
+ * gpe_norm_noalloc -- no counterpart in the reference.  The same weighted
+ * integral as gpe_norm (extended closed quadrature times dx*dy*dz), for a
+ * caller-owned device array, without allocating any device memory.
+ *
+ * For callers that cannot let a library allocate on the GPU: hosts whose
+ * device memory is owned by another allocator (a framework's caching pool,
+ * a runtime that maps its own buffers) and must not see foreign
+ * cudaMalloc/cudaFree traffic; loops that must not stall or fail on an
+ * allocation between steps; embedders that fix their device-memory budget
+ * up front.  The caller passes the input (contiguous interior psi in the
+ * reference's order, complex128 or complex64 by dtype) and the output (one
+ * double in device memory); the work is queued on `stream` (NULL = the
+ * legacy default stream) and the call does not wait for it.
+ *
+ * Scratch: one partial sum per z-plane in a fixed array inside the library
+ * (GPE_NOALLOC_MAX_NZ doubles, 64 KiB), resident on every GPU that loads the
+ * library until the process exits.  nz > GPE_NOALLOC_MAX_NZ (or nx, ny,
+ * nz < 6, a bad dtype, a NULL pointer) returns GPE_ERR_BADARG and prints the
+ * reason on stderr.  The first call on a device looks up the array's device
+ * address (and so loads the module there); make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller.
+ */
+#define GPE_NOALLOC_MAX_NZ 8192
+int gpe_norm_noalloc(const void* psi_dev, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
+                     double dz, double* norm_dev, void* stream);
+
 /* Library build/version string. */
 const char* gpe_version(void);
 
