@@ -186,6 +186,142 @@ def run_reference(args, ws, rank):
     return 0
 
 
+def read_profile(s):
+    """Per-kind (total ms, launches, B/site) from the library's event timing."""
+    import ctypes as C
+
+    from gpe_b200 import _lib as L
+
+    prof = {}
+    for kind, name in enumerate(L.KIND_NAMES):
+        tot, n, bps = C.c_double(), C.c_int64(), C.c_double()
+        s.lib.gpe_profile_get(s.h, kind, C.byref(tot), C.byref(n), C.byref(bps))
+        if n.value:
+            prof[name] = (tot.value, n.value, bps.value)
+    return prof
+
+
+def fp32_storage_leg(args, torch, psi0):
+    """The same 256^3 workload with complex64 storage (FP32 stencil, FP64
+    stage combinations and reductions): device-resident site-updates/s."""
+    from gpe_b200.solver import RunParams, Solver
+
+    out = {}
+    for compute in ("f32", "f64"):
+        rp = RunParams(**WORKLOAD, storage="c64", compute=compute)
+        s = Solver(rp)
+        s.set_state(psi0)
+        stream = torch.cuda.ExternalStream(s.stream())
+        for _ in range(max(1, args.warmup)):
+            s.solver(CHUNK, wait=False)
+        s.sync()
+        s.lib.gpe_profile(s.h, 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = max(1, args.steps // 2)
+        e0.record(stream)
+        for _ in range(n):
+            s.solver(CHUNK, wait=False)
+        e1.record(stream)
+        s.sync()
+        ms = e0.elapsed_time(e1)
+        prof = read_profile(s)
+        s.close()
+        n_sites = rp.nx * rp.ny * rp.nz
+        tot, cnt, bps = prof["rk4_23"]
+        out[compute + "_compute"] = {
+            "value": n_sites * CHUNK * n / (ms * 1e-3), "unit": UNIT, "bytes_per_site_step": 128,
+            "stage23_gbs": bps * n_sites / (tot / cnt * 1e-3) / 1e9,
+            "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()}}
+    return out
+
+
+def rk45_leg(args, torch):
+    """Trapped-condensate RKF45 workload: 192x192x384, dx = 0.25, reflective,
+    4th order, eqn 4 with damping gamma = 0.05, mu = 10, trap (0.05, 0.05,
+    0.025), TF x Pade vortex line, eps = 1e-6, complex128.  Site-updates/s
+    count accepted steps; each attempt moves 576 B/site."""
+    from gpe_b200 import ic
+    from gpe_b200.solver import RunParams, Solver
+
+    rp = RunParams(nx=192, ny=192, nz=384, xr=23.875, yr=23.875, zr=47.875, tau=0.01, scheme="rk45",
+                   eqn_to_solve=4, bcs=2, order=4, g=1.0, mu=10.0, omx=0.05, omy=0.05, omz=0.025, gamma=0.05)
+    psi0 = ic.fermi(rp) * ic.vortex_line_pade(rp, dir="z")
+    s = Solver(rp)
+    s.set_state(psi0)
+    s.solver(10)  # settle the adaptive step
+    s.lib.gpe_profile(s.h, 1)
+    per = 20
+    t0 = time.perf_counter()
+    acc = rej = 0
+    for _ in range(max(1, args.steps // 2)):
+        info = s.solver(per)
+        acc += info.accepted
+        rej += info.rejected
+    wall = time.perf_counter() - t0
+    prof = read_profile(s)
+    dev_ms = sum(v[0] for v in prof.values())
+    attempts = acc + rej
+    n_sites = rp.nx * rp.ny * rp.nz
+    s.close()
+    return {"value": n_sites * acc / wall, "unit": UNIT, "accepted": acc, "rejected": rej,
+            "dt_last": abs(s.dt), "device_ms_per_attempt": dev_ms / attempts,
+            "device_gbs": 576 * n_sites * attempts / (dev_ms * 1e-3) / 1e9,
+            "timing": "wall clock around gpe_step (includes the 8-byte error-norm read-back per attempt)"}
+
+
+C4_STEPS = 500
+
+
+def batched_leg(args, torch):
+    """64 independent solves in one pool: cubic sizes uniform in
+    {32, 48, ..., 160}, periodic/reflective and 2nd/4th order mixed (seeded),
+    RK4 dt = 0.01, 500 steps, ring (r0 in [2,6]) / random-phase (cutoff in
+    [1,2]) initial states alternating, complex64 storage with FP64
+    reductions, tile_zc per size from the autotuner.  Timed on the host clock
+    from the first submission to the last retired result (state upload and
+    download included); latencies are per solve, all submitted at t = 0."""
+    from gpe_b200 import autotune
+    from gpe_b200 import ic
+    from gpe_b200.pool import Pool
+    from gpe_b200.solver import RunParams
+
+    rng = np.random.default_rng(64)
+    cache = autotune.load_cache()
+    solves = []
+    for k in range(64):
+        n = int(rng.choice(np.arange(32, 161, 16)))
+        bcs, order = int(rng.choice([1, 2])), int(rng.choice([2, 4]))
+        r0, kc = float(rng.uniform(2, 6)), float(rng.uniform(1, 2))
+        h = 0.25 * (n - 1)
+        rp = RunParams(nx=n, ny=n, nz=n, xr=h, yr=h, zr=h, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=bcs,
+                       order=order, g=1.0, mu=1.0, storage="c64",
+                       tile_zc=autotune.best_zc(n, order, "c64", cache))
+        psi = ic.vortex_ring(rp, "xy", r0=r0) if k % 2 == 0 else ic.random_phase(rp, seed=k, kc=kc)
+        solves.append((rp, psi.astype(np.complex64)))
+    autotune.save_cache(cache)
+    budget = sum(Pool.solve_bytes(rp) for rp, _ in solves) + (256 << 20)
+    warm = Pool(budget)
+    for k, (rp, psi) in enumerate(solves):
+        warm.submit(rp, psi, 2, k)
+    warm.run_all()
+    warm.close()
+    pool = Pool(budget)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k, (rp, psi) in enumerate(solves):
+        assert pool.submit(rp, psi, C4_STEPS, k)
+    res = pool.run_all(max_steps=C4_STEPS)
+    wall = time.perf_counter() - t0
+    pool.close()
+    sites = sum(rp.nx * rp.ny * rp.nz for rp, _ in solves)
+    lat = np.array([r.finish_s - r.submit_s for r in res])
+    return {"value": sites * C4_STEPS / wall, "unit": UNIT, "solves": len(res), "sites": sites,
+            "steps": C4_STEPS, "wall_s": wall, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "storage": "c64",
+            "tile_zc": {k: v["zc"] for k, v in cache.items()},
+            "timing": "host clock, first submit to last result, uploads/downloads included"}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,6 +330,7 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="device-resident leg only (tuning sweeps)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP32-storage and RKF45 legs")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling target: set up the workload and run 2 RK4 steps, nothing else")
     args = ap.parse_args()
@@ -248,14 +385,7 @@ def main() -> int:
     value = n_sites * CHUNK * args.steps * ws / (ms * 1e-3)
     gpu_launches = 4 * CHUNK * args.steps
 
-    import ctypes as C
-
-    prof = {}
-    for kind, name in enumerate(L.KIND_NAMES):
-        tot, n, bps = C.c_double(), C.c_int64(), C.c_double()
-        s.lib.gpe_profile_get(s.h, kind, C.byref(tot), C.byref(n), C.byref(bps))
-        if n.value:
-            prof[name] = (tot.value, n.value, bps.value)
+    prof = read_profile(s)
     s.lib.gpe_profile(s.h, 0)
 
     # roofline of the dominant kernel: the RK4 stage-2/3 kernel (80 B/site)
@@ -311,6 +441,12 @@ def main() -> int:
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
             "e2e": e2e, "roofline": roofline, "clocks": clk.summary(), "gpu_launches": gpu_launches}
+    if not args.no_extras:
+        line["fp32_storage"] = fp32_storage_leg(args, torch, psi0)
+        line["fp32_storage"]["speedup_vs_fp64"] = line["fp32_storage"]["f32_compute"]["value"] / (value / ws)
+        line["rk45_trapped"] = rk45_leg(args, torch)
+        line["batched_c4"] = batched_leg(args, torch)
+        line["batched_c4"]["speedup_vs_plain_fp64"] = line["batched_c4"]["value"] / (value / ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     s.close()

@@ -33,6 +33,7 @@ class GpeParams(C.Structure):
         ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
         ("scheme", C.c_int32), ("eqn", C.c_int32), ("bcs", C.c_int32), ("order", C.c_int32),
         ("real_time", C.c_int32), ("storage", C.c_int32), ("compute", C.c_int32),
+        ("tile_zc", C.c_int32), ("reserved", C.c_int32),
         ("xr", C.c_double), ("yr", C.c_double), ("zr", C.c_double),
         ("tau", C.c_double),
         ("Urhs", C.c_double), ("diss_amp", C.c_double), ("scal", C.c_double), ("g", C.c_double),
@@ -49,6 +50,15 @@ class GpeStepInfo(C.Structure):
         ("p", C.c_int64), ("accepted", C.c_int64), ("rejected", C.c_int64),
         ("errmax", C.c_double), ("norm", C.c_double), ("energy", C.c_double),
         ("want_norm", C.c_int32), ("want_energy", C.c_int32),
+    ]
+
+
+class GpeResult(C.Structure):
+    _fields_ = [
+        ("tag", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_int32),
+        ("steps", C.c_int64), ("rejected", C.c_int64),
+        ("t", C.c_double), ("im_t", C.c_double), ("dt_re", C.c_double), ("dt_im", C.c_double),
+        ("norm", C.c_double), ("submit_s", C.c_double), ("start_s", C.c_double), ("finish_s", C.c_double),
     ]
 
 
@@ -73,6 +83,15 @@ _PROTOS = {
     "gpe_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "gpe_profile_get": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                   C.POINTER(C.c_double)]),
+    "gpe_pool_create": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
+    "gpe_pool_submit": (C.c_int, [C.c_void_p, C.POINTER(GpeParams), C.c_void_p, C.c_int32, C.c_int64, C.c_uint64,
+                                  C.c_void_p]),
+    "gpe_pool_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
+    "gpe_pool_poll": (C.c_int, [C.c_void_p, C.POINTER(GpeResult), C.c_int32, C.POINTER(C.c_int32)]),
+    "gpe_pool_free_bytes": (C.c_int64, [C.c_void_p]),
+    "gpe_pool_solve_bytes": (C.c_int64, [C.POINTER(GpeParams)]),
+    "gpe_pool_last_error": (C.c_char_p, [C.c_void_p]),
+    "gpe_pool_destroy": (None, [C.c_void_p]),
     "gpe_norm_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
 }

@@ -1,0 +1,80 @@
+"""Tile-shape autotuner: for each (grid size, FD order, storage) pick the
+number of z planes per CTA work item (tile_zc) that gives the fastest RK4
+step, by timing candidates on the GPU; results are cached in a JSON file so
+a size is measured once per machine.
+
+The x-y tile is fixed by the TMA box (32 x 8 sites); tile_zc trades the
+z-halo re-read (2R planes per item) against the number of items, which
+matters most for the small and uneven grids of a batched workload.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+from .solver import RunParams, Solver
+
+CACHE = Path(os.environ.get("GPE_TUNE_CACHE", Path(__file__).resolve().parent / "tune_cache.json"))
+CANDIDATES = (4, 8, 16, 32)
+
+
+def _key(n: int, order: int, storage: str) -> str:
+    return f"n{n}_o{order}_{storage}"
+
+
+def load_cache() -> dict:
+    try:
+        return json.loads(CACHE.read_text())
+    except Exception:
+        return {}
+
+
+def save_cache(c: dict) -> None:
+    CACHE.write_text(json.dumps(c, indent=1, sort_keys=True) + "\n")
+
+
+def time_rk4(rp: RunParams, steps: int = 20) -> float:
+    """Seconds per RK4 step of one solve (CUDA events on its stream)."""
+    import torch
+
+    s = Solver(rp)
+    s.set_state(np.ones((rp.nz, rp.ny, rp.nx), np.complex128))
+    st = torch.cuda.ExternalStream(s.stream())
+    s.solver(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.solver(steps, wait=False)
+    e1.record(st)
+    s.sync()
+    t = e0.elapsed_time(e1) * 1e-3 / steps
+    s.close()
+    return t
+
+
+def best_zc(n: int, order: int, storage: str, cache: dict | None = None) -> int:
+    """Tuned tile_zc for a cubic n^3 grid (measures on a cache miss)."""
+    own = cache is None
+    cache = load_cache() if cache is None else cache
+    k = _key(n, order, storage)
+    if k not in cache:
+        h = 0.25 * (n - 1)
+        base = RunParams(nx=n, ny=n, nz=n, xr=h, yr=h, zr=h, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=1,
+                         order=order, storage=storage)
+        times = {zc: time_rk4(base.replace(tile_zc=zc)) for zc in CANDIDATES if zc <= n}
+        cache[k] = {"zc": min(times, key=times.get), "s_per_step": times}
+        if own:
+            save_cache(cache)
+    return int(cache[k]["zc"])
+
+
+def tune(sizes, orders=(2, 4), storages=("c64",)) -> dict:
+    cache = load_cache()
+    for n in sizes:
+        for o in orders:
+            for st in storages:
+                best_zc(n, o, st, cache)
+    save_cache(cache)
+    return cache

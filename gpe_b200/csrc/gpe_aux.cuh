@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) k_norm(const S* __restrict__ f, Geom g, i
 }
 
 // Sum (slots 0,1) and max (slot 2) of nb block partials in a fixed order.
-__global__ void __launch_bounds__(256) k_finalize(const double* __restrict__ partials, long long nb, double* out) {
+static __global__ void __launch_bounds__(256) k_finalize(const double* __restrict__ partials, long long nb, double* out) {
   __shared__ double s0[256], s1[256], s2[256];
   const int t = threadIdx.x;
   double a = 0.0, b = 0.0, c = 0.0;
@@ -90,6 +90,59 @@ __global__ void __launch_bounds__(256) k_finalize(const double* __restrict__ par
     out[0] = s0[0];
     out[1] = s1[0];
     out[2] = s2[0];
+  }
+}
+
+// Per-solve sums of work-item partials: block s reduces items
+// [first[s], first[s+1]) in a fixed order (thread-strided, then a tree), so a
+// solve's result depends only on its own items.
+static __global__ void __launch_bounds__(256) k_finalize_ranges(const double* __restrict__ partials,
+                                                         const int* __restrict__ first, double* out) {
+  __shared__ double s0[256], s1[256], s2[256];
+  const int sv = blockIdx.x, t = threadIdx.x;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int q = first[sv] + t; q < first[sv + 1]; q += 256) {
+    a += partials[(long long)q * RED_SLOTS + 0];
+    b += partials[(long long)q * RED_SLOTS + 1];
+    c = fmax(c, partials[(long long)q * RED_SLOTS + 2]);
+  }
+  s0[t] = a;
+  s1[t] = b;
+  s2[t] = c;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w) {
+      s0[t] += s0[t + w];
+      s1[t] += s1[t + w];
+      s2[t] = fmax(s2[t], s2[t + w]);
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    out[sv * RED_SLOTS + 0] = s0[0];
+    out[sv * RED_SLOTS + 1] = s1[0];
+    out[sv * RED_SLOTS + 2] = s2[0];
+  }
+}
+
+// Face ghosts of a field whose interior was just written (for example by a
+// strided host-to-device copy): every interior site writes its ghost copies.
+template <class S>
+__global__ void k_fill_ghosts(S* f, Geom g, int R, int bcs) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx);
+    const long long r = t / g.nx;
+    const int j = (int)(r % g.ny);
+    const int k = (int)(r / g.ny);
+    const int gx = ghost_pos(i, g.nx, R, bcs), gy = ghost_pos(j, g.ny, R, bcs), gz = ghost_pos(k, g.nz, R, bcs);
+    if (gx == NOGHOST && gy == NOGHOST && gz == NOGHOST) continue;
+    const long long col = (long long)(j + 2) * g.px + g.xoff + i;
+    const long long pl = (long long)(k + 2) * g.pz;
+    const S v = f[pl + col];
+    if (gx != NOGHOST) f[pl + (long long)(j + 2) * g.px + g.xoff + gx] = v;
+    if (gy != NOGHOST) f[pl + (long long)(gy + 2) * g.px + g.xoff + i] = v;
+    if (gz != NOGHOST) f[(long long)(gz + 2) * g.pz + col] = v;
   }
 }
 

@@ -20,6 +20,7 @@
 #include "gpe_aux.cuh"
 #include "gpe_device.cuh"
 #include "gpe_stage_tma.cuh"
+#include "gpe_common.h"
 
 namespace gpe {
 cudaError_t launch_stage_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
@@ -34,6 +35,7 @@ cudaError_t launch_stage_tma_f32x(int kind, int R, int ty, dim3 grid, cudaStream
 }  // namespace gpe
 
 using namespace gpe;
+using gpe::CK_B;
 
 namespace {
 
@@ -41,15 +43,6 @@ thread_local std::string g_create_err;
 
 enum { CM_F64 = 0, CM_F32 = 1, CM_F32X = 2 };
 enum { T_VX, T_VY, T_VZ, T_SX, T_SY, T_SZ, T_WX, T_WY, T_WZ, T_CX, T_CY, T_CZ, T_NUM };
-
-// Cash-Karp tableau (src/solve.f90:255-269)
-const double CK_B[5][5] = {
-    {0.2, 0, 0, 0, 0},
-    {0.075, 0.225, 0, 0, 0},
-    {0.3, -0.9, 1.2, 0, 0},
-    {-11.0 / 54.0, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0},
-    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0},
-};
 
 }  // namespace
 
@@ -106,92 +99,12 @@ int fail(gpe_handle* h, int code, const std::string& msg) {
                                          " at " #call);                                    \
   } while (0)
 
-int validate(const gpe_params* p, std::string& why) {
-  if (!p) { why = "null parameters"; return GPE_ERR_BADARG; }
-  if (p->nx < 6 || p->ny < 6 || p->nz < 6) { why = "nx, ny, nz must be >= 6"; return GPE_ERR_BADARG; }
-  if (p->scheme < GPE_EULER || p->scheme > GPE_RK45) {
-    why = "ERROR: Unrecognised time stepping scheme.";  // src/solve.f90:49
-    return GPE_ERR_BADARG;
-  }
-  if (p->eqn < 1 || p->eqn > 4) { why = "eqn_to_solve must be 1..4"; return GPE_ERR_BADARG; }
-  if (p->bcs != 1 && p->bcs != 2) { why = "bcs must be 1 (periodic) or 2 (reflective)"; return GPE_ERR_BADARG; }
-  if (p->order != 2 && p->order != 4) { why = "order must be 2 or 4"; return GPE_ERR_BADARG; }
-  if (p->storage != GPE_C128 && p->storage != GPE_C64) { why = "storage must be GPE_C128 or GPE_C64"; return GPE_ERR_BADARG; }
-  if (!(p->xr > 0 && p->yr > 0 && p->zr > 0)) { why = "xr, yr, zr must be > 0"; return GPE_ERR_BADARG; }
-  if (!(p->tau > 0) || !std::isfinite(p->tau)) { why = "tau must be > 0"; return GPE_ERR_BADARG; }
-  return GPE_OK;
-}
-
-void layout(const gpe_params* p, Geom& g, int& esz) {
-  esz = p->storage == GPE_C128 ? 16 : 8;
-  g.nx = p->nx;
-  g.ny = p->ny;
-  g.nz = p->nz;
-  g.xoff = 128 / esz;
-  const long long need = g.xoff + (long long)p->nx + 2;
-  g.px = (need + g.xoff - 1) / g.xoff * g.xoff;
-  g.pz = (long long)(p->ny + 4) * g.px;
-}
-
-long long padded_elems(const Geom& g) { return (long long)(g.nz + 4) * g.pz; }
-
-int nfields(int scheme) {
-  switch (scheme) {
-    case GPE_EULER: return 2;
-    case GPE_RK2: return 2;
-    case GPE_RK4: return 4;
-    default: return 9;  // psi, psi_new, A, B, K1..K5
-  }
-}
-
-// z planes per block: enough blocks for several waves on 148 SMs
-int choose_zc(const Geom& g) {
-  if (const char* e = getenv("GPE_ZC")) {
-    int v = atoi(e);
-    if (v > 0) return std::min(v, g.nz);
-  }
-  // 16 planes per CTA measured best at 256^3 (TMA kernel, sweep 8..64);
-  // small grids use fewer so that every SM gets several CTAs.
-  const long long bxy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
-  const long long target = 148LL * 8;
-  long long zc = (g.nz * bxy + target - 1) / target;
-  zc = std::max<long long>(4, std::min<long long>(zc, 16));
-  return (int)std::min<long long>(zc, g.nz);
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
-  return fn;
-}
-
-// Tensor maps of one ghost-padded field: rank 3 over (2*px scalars, ny+4
-// rows, nz+4 planes); box = halo'd stencil tile or plain point-wise tile.
+int validate(const gpe_params* p, std::string& why) { return validate_params(p, why); }
+void layout(const gpe_params* p, Geom& g, int& esz) { param_layout(p, g, esz); }
+int nfields(int scheme) { return scheme_fields(scheme); }
+int choose_zc(const Geom& g) { return default_zc(g); }
 bool encode_field_maps(gpe_handle* h, void* base, CUtensorMap* halo, CUtensorMap* pw) {
-  auto enc = tensor_map_encoder();
-  if (!enc) return false;
-  const Geom& g = h->g;
-  const CUtensorMapDataType dt = h->esz == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  const cuuint64_t dims[3] = {(cuuint64_t)(2 * g.px), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
-  const cuuint64_t strides[2] = {(cuuint64_t)(g.px * h->esz), (cuuint64_t)(g.pz * h->esz)};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint32_t box_h[3] = {(cuuint32_t)(2 * tma_stencil_w()), (cuuint32_t)tma_stencil_h(8, h->R), 1};
-  const cuuint32_t box_p[3] = {(cuuint32_t)(2 * TMA_TX), 8, 1};
-  if (enc(halo, dt, 3, base, dims, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return false;
-  if (enc(pw, dt, 3, base, dims, strides, box_p, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-    return false;
-  return true;
+  return encode_maps(base, h->g, h->esz, h->R, halo, pw);
 }
 
 int field_of(const gpe_handle* h, const void* p) {
@@ -268,108 +181,18 @@ void prof_resolve(gpe_handle* h) {
   h->ev_used = 0;
 }
 
-// algorithmic HBM traffic of one launch of a stage kind, in field elements
-// per site: one read of every input field and one write of every output
-// field (stencil neighbours come from on-chip reuse)
-int kind_elems(int kind) {
-  switch (kind) {
-    case K_EULER: return 2;
-    case K_RK2_1: return 2;
-    case K_RK2_2: return 3;
-    case K_RK4_1: return 3;
-    case K_RK4_2: return 5;
-    case K_RK4_4: return 3;
-    case K_CK_1: return 3;
-    case K_CK_2: return 5;
-    case K_CK_3: return 6;
-    case K_CK_4: return 7;
-    case K_CK_5: return 8;
-    case K_CK_6: return 7;
-    case K_ENERGY: return 1;
-    default: return 0;
-  }
-}
-
-// host tables and grid (src/ic.f90:32-69, solve.f90:397-409, ic.f90:713-731,
-// variables.f90:49-51 + 730-840)
 void build_tables(gpe_handle* h, std::vector<double>& t) {
-  const gpe_params& p = h->p;
-  const int n[3] = {p.nx, p.ny, p.nz};
-  const double r[3] = {p.xr, p.yr, p.zr};
-  const double om[3] = {p.omx, p.omy, p.omz};
-  std::vector<double>* c[3] = {&h->x, &h->y, &h->z};
-  double* d[3] = {&h->dx, &h->dy, &h->dz};
-  const double QC1 = 3.0 / 8.0, QC2 = 7.0 / 6.0, QC3 = 23.0 / 24.0;
-  const size_t ntot = (size_t)p.nx + p.ny + p.nz;
-  t.assign(ntot * 4, 0.0);
-  size_t off = 0;
-  for (int ax = 0; ax < 3; ++ax) {
-    const double lo = -r[ax];
-    *d[ax] = (r[ax] - lo) / (n[ax] - 1);
-    c[ax]->resize(n[ax]);
-    for (int q = 0; q < n[ax]; ++q) (*c[ax])[q] = lo + (double)q * *d[ax];
-    const double a = (*c[ax])[n[ax] - 3];
-    for (int q = 0; q < n[ax]; ++q) {
-      const double xq = (*c[ax])[q];
-      t[0 * ntot + off + q] = (om[ax] * om[ax]) * (xq * xq);
-      t[1 * ntot + off + q] = 1.0 + tanh(xq - a) * tanh(xq + a);
-      double w = 1.0;
-      if (q == 0) w = QC1;
-      if (q == 1) w = QC2;
-      if (q == 2) w = QC3;
-      if (q == n[ax] - 3) w = QC3;
-      if (q == n[ax] - 2) w = QC2;
-      if (q == n[ax] - 1) w = QC1;
-      t[2 * ntot + off + q] = w;
-      t[3 * ntot + off + q] = xq;
-    }
-    off += n[ax];
-  }
+  std::vector<double>* xyz[3] = {&h->x, &h->y, &h->z};
+  double d[3];
+  build_axis_tables(h->p, t, xyz, d);
+  h->dx = d[0];
+  h->dy = d[1];
+  h->dz = d[2];
 }
 
 StageArgs base_args(gpe_handle* h) {
-  StageArgs a;
-  memset(&a, 0, sizeof(a));
-  const gpe_params& p = h->p;
-  a.g = h->g;
-  a.bcs = p.bcs;
-  a.eqn = p.eqn;
-  a.zc = h->zc;
-  a.has_urhs = (p.Urhs != 0.0) && p.eqn != 4;
-  a.has_diss = (p.diss_amp != 0.0) && (p.eqn == 1 || p.eqn == 3);
-  const double dx2 = h->dx * h->dx, dy2 = h->dy * h->dy, dz2 = h->dz * h->dz;
-  if (p.order == 2) {
-    a.ixx = 1.0 / dx2;
-    a.iyy = 1.0 / dy2;
-    a.izz = 1.0 / dz2;
-    a.ix1 = 1.0 / (2.0 * h->dx);
-  } else {
-    a.ixx = 1.0 / (12.0 * dx2);
-    a.iyy = 1.0 / (12.0 * dy2);
-    a.izz = 1.0 / (12.0 * dz2);
-    a.ix1 = 1.0 / (12.0 * h->dx);
-  }
-  a.g_nl = p.g;
-  a.mu = p.mu;
-  a.gamma = p.eqn == 4 ? p.gamma : 0.0;
-  a.urhs = p.Urhs;
-  a.diss_amp = p.diss_amp;
-  const size_t ntot = (size_t)p.nx + p.ny + p.nz;
-  const double* T = h->tables;
-  const double* blk[4] = {T, T + ntot, T + 2 * ntot, T + 3 * ntot};
-  a.vx = blk[0];
-  a.vy = blk[0] + p.nx;
-  a.vz = blk[0] + p.nx + p.ny;
-  a.sx = blk[1];
-  a.sy = blk[1] + p.nx;
-  a.sz = blk[1] + p.nx + p.ny;
-  a.wx = blk[2];
-  a.wy = blk[2] + p.nx;
-  a.wz = blk[2] + p.nx + p.ny;
-  a.cx = blk[3];
-  a.cy = blk[3] + p.nx;
-  a.cz = blk[3] + p.nx + p.ny;
-  return a;
+  const double d[3] = {h->dx, h->dy, h->dz};
+  return make_base_args(h->p, h->g, h->R, h->zc, d, h->tables);
 }
 
 int finalize_into(gpe_handle* h, const double* part, int slot) {
@@ -653,7 +476,7 @@ int gpe_create(const gpe_params* p, gpe_handle** out) {
   h->R = p->order / 2;
   h->cmode = p->storage == GPE_C128 ? CM_F64 : (p->compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32);
   h->nelem = padded_elems(h->g);
-  h->zc = choose_zc(h->g);
+  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, p->nz) : choose_zc(h->g);
   h->grid = dim3((p->nx + 31) / 32, (p->ny + 7) / 8, (p->nz + h->zc - 1) / h->zc);
   h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
   auto bail = [&](int rc) {

@@ -52,6 +52,7 @@ struct Geom {
 
 struct StageArgs {
   Geom g;
+  int R;                // stencil radius: 1 (order 2) or 2 (order 4)
   int bcs;              // 1 periodic, 2 reflective
   int eqn;              // 1..4
   int zc;               // z planes per block
@@ -235,10 +236,32 @@ __device__ __forceinline__ void store_with_ghosts(S* f, const Geom& g, long long
   if (gz != NOGHOST) f[(long long)(gz + 2) * g.pz + col] = v;
 }
 
+// Same with the centre offset o of (i,j,k) already known.
+template <class S>
+__device__ __forceinline__ void store_at(S* f, const Geom& g, long long o, int i, int j, int k, int gx, int gy,
+                                         int gz, S v) {
+  f[o] = v;
+  if (gx != NOGHOST) f[o + (gx - i)] = v;
+  if (gy != NOGHOST) f[o + (long long)(gy - j) * g.px] = v;
+  if (gz != NOGHOST) f[o + (long long)(gz - k) * g.pz] = v;
+}
+
 // Deterministic block sum of up to RED_SLOTS values (fixed shuffle and warp
 // order), thread 0 writes the block's partials.  Slot RED_ERR is a max.
 template <int NT>
+__device__ __forceinline__ void block_reduce_store_at(double v0, double v1, double v2, double* partials,
+                                                      long long b);
+
+template <int NT>
 __device__ __forceinline__ void block_reduce_store(double v0, double v1, double v2, double* partials) {
+  const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+  block_reduce_store_at<NT>(v0, v1, v2, partials, b);
+}
+
+// Same, writing the partials of slot b (a work-item index in batched launches).
+template <int NT>
+__device__ __forceinline__ void block_reduce_store_at(double v0, double v1, double v2, double* partials,
+                                                      long long b) {
   __shared__ double red[NT / 32][RED_SLOTS];
   const int tid = threadIdx.x + threadIdx.y * blockDim.x;
 #pragma unroll
@@ -260,7 +283,6 @@ __device__ __forceinline__ void block_reduce_store(double v0, double v1, double 
       s1 += red[w][1];
       s2 = fmax(s2, red[w][2]);
     }
-    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
     partials[b * RED_SLOTS + 0] = s0;
     partials[b * RED_SLOTS + 1] = s1;
     partials[b * RED_SLOTS + 2] = s2;
@@ -309,10 +331,11 @@ __device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i,
 // right-hand side, the stage combination, the stores (with ghosts) and the
 // fused reductions.  pw[] holds the point-wise inputs in the order
 // psi, acc, K... of StageTraits.
+// o is the element offset of (i,j,k); gz = ghost_pos(k, nz, R, bcs).
 template <class S, class C, int R, int KIND>
 __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, const S* pw, int i, int j, int k,
-                                           long long col, const ColumnConsts& cc, double& r_norm, double& r_en,
-                                           double& r_err) {
+                                           long long o, int gz, const ColumnConsts& cc, double& r_norm,
+                                           double& r_en, double& r_err) {
   using T = StageTraits<KIND>;
   const Geom& g = a.g;
   const cx<C> lxx = d2<C, R>(n.xm2, n.xm1, n.c0, n.xp1, n.xp2, (C)a.ixx);
@@ -322,8 +345,6 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
   lap.r = (lxx.r + lyy.r) + lzz.r;
   lap.i = (lxx.i + lyy.i) + lzz.i;
 
-  const int gz = ghost_pos(k, g.nz, R, a.bcs);
-  const long long o = (long long)(k + 2) * g.pz + col;
   const double cr = (double)n.c0.r, ci = (double)n.c0.i;
 
   if constexpr (T::FIRST) {
@@ -355,7 +376,7 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
       else base = cx<double>{cr, ci};
       const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
       const S ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
-      store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, ns);
+      store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
       if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
         // acc = (psi | acc) + cf1 * f
         const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
@@ -385,7 +406,7 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
         }
         tr = tr + a.b[T::NK] * Kmd.r;
         ti = ti + a.b[T::NK] * Kmd.i;
-        store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<double>{tr, ti}));
+        store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<double>{tr, ti}));
       } else {
         // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
         // contribute exact zeros and are skipped.
@@ -397,7 +418,7 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
         const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
         const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
         const S ns = to_s<S>(cx<double>{nr, ni});
-        store_with_ghosts(out, g, col, i, j, k, cc.gx, cc.gy, gz, ns);
+        store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
         const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
         const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
         // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
@@ -542,7 +563,8 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
       } else {
         n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
       }
-      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, col, cc, r_norm, r_en, r_err);
+      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, (long long)(k + 2) * g.pz + col, ghost_pos(k, g.nz, R, a.bcs),
+                                cc, r_norm, r_en, r_err);
     }
 
     // rotate the queue

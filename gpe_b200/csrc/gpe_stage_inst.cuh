@@ -38,7 +38,7 @@ static cudaError_t launch_kind(int kind, dim3 grid, cudaStream_t st, const Stage
 
 template <class S, class C, int R, int K, int TY>
 static cudaError_t launch_tma_one(dim3 grid, cudaStream_t st, const TmaMaps& m, const StageArgs& a) {
-  using LY = TmaLayout<S, R, K, TY>;
+  using LY = TmaLayout<S, R, StageTraits<K>::NPW, TY>;
   static unsigned long long attr_set = 0;  // per instantiation, one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
@@ -86,6 +86,64 @@ static cudaError_t launch_stage_tma_impl(int kind, int R, int ty, dim3 grid, cud
   return cudaErrorInvalidValue;
 }
 
+// Opt the batched kernel into its dynamic shared memory once per device and
+// cache how many of its CTAs fit on the device at once.
+template <class S, class C, int K>
+static cudaError_t batch_setup(int* occupancy) {
+  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
+  static unsigned long long done = 0;
+  static int occ[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64) return cudaErrorInvalidDevice;
+  if (!(done & (1ULL << dev))) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_stage_batch<S, C, K, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
+    if (e != cudaSuccess) return e;
+    int nsm = 0, per = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8>, 256, LY::SMEM);
+    if (e != cudaSuccess) return e;
+    occ[dev] = nsm * (per > 0 ? per : 1);
+    done |= 1ULL << dev;
+  }
+  if (occupancy) *occupancy = occ[dev];
+  return cudaSuccess;
+}
+
+template <class S, class C, int K>
+static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+                                    int nitems, double* partials) {
+  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
+  cudaError_t e = batch_setup<S, C, K>(nullptr);
+  if (e != cudaSuccess) return e;
+  k_stage_batch<S, C, K, 8><<<grid, dim3(32, 8), LY::SMEM, st>>>(tab, items, nitems, partials);
+  return cudaGetLastError();
+}
+
+template <class S, class C>
+static cudaError_t launch_batch_impl(int kind, int grid, cudaStream_t st, const BatchStage* tab,
+                                     const BatchItem* items, int nitems, double* partials, int* occupancy) {
+  switch (kind) {
+#define GPE_BCASE(K)                                                       \
+  case K:                                                                  \
+    if (grid <= 0) return batch_setup<S, C, K>(occupancy);               \
+    return launch_batch_one<S, C, K>(grid, st, tab, items, nitems, partials);
+    GPE_BCASE(K_RK4_1)
+    GPE_BCASE(K_RK4_2)
+    GPE_BCASE(K_RK4_4)
+    GPE_BCASE(K_CK_1)
+    GPE_BCASE(K_CK_2)
+    GPE_BCASE(K_CK_3)
+    GPE_BCASE(K_CK_4)
+    GPE_BCASE(K_CK_5)
+    GPE_BCASE(K_CK_6)
+#undef GPE_BCASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 template <class S, class C>
 static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a) {
   if (ty != 8) return cudaErrorInvalidValue;
@@ -104,5 +162,9 @@ static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStr
   cudaError_t launch_stage_tma_##TAG(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m, \
                                      const StageArgs& a) {                                              \
     return launch_stage_tma_impl<S, C>(kind, R, ty, grid, st, m, a);                                    \
+  }                                                                                                     \
+  cudaError_t launch_batch_##TAG(int kind, int grid, cudaStream_t st, const BatchStage* tab,            \
+                                 const BatchItem* items, int nitems, double* partials, int* occupancy) { \
+    return launch_batch_impl<S, C>(kind, grid, st, tab, items, nitems, partials, occupancy);            \
   }                                                                                                     \
   }

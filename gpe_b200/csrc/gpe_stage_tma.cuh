@@ -86,84 +86,115 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-template <class S, int R, int KIND, int TY>
+template <class S>
+__host__ __device__ constexpr uint32_t tma_st_bytes(int R, int TY) {
+  return (uint32_t)(tma_stencil_w() * (TY + 2 * R) * sizeof(S));
+}
+template <class S>
+__host__ __device__ constexpr uint32_t tma_pw1_bytes(int TY) {
+  return (uint32_t)(TMA_TX * TY * sizeof(S));
+}
+__host__ __device__ constexpr uint32_t round128(uint32_t b) { return (b + 127) / 128 * 128; }
+
+// Shared-memory layout of the two rings.  RMAX sizes the stencil slots (a
+// batched launch mixes R = 1 and R = 2 solves in the same rings).
+template <class S, int RMAX, int NPW, int TY>
 struct TmaLayout {
-  static constexpr int NPW = StageTraits<KIND>::NPW;
-  static constexpr int NSS = 2 * R + 2;                       // stencil ring slots
-  static constexpr int NPS = 3;                               // point-wise ring slots
-  static constexpr uint32_t ST_BYTES = tma_stencil_w() * (TY + 2 * R) * sizeof(S);
-  static constexpr uint32_t PW1_BYTES = TMA_TX * TY * sizeof(S);
-  static constexpr uint32_t ST_SLOT = (ST_BYTES + 127) / 128 * 128;
-  static constexpr uint32_t PW_SLOT = (NPW * PW1_BYTES + 127) / 128 * 128;
+  static constexpr int NSS = 2 * RMAX + 2;  // stencil ring slots
+  static constexpr int NPS = 3;             // point-wise ring slots
+  static constexpr uint32_t ST_SLOT = round128(tma_st_bytes<S>(RMAX, TY));
+  static constexpr uint32_t PW_SLOT = round128(NPW * tma_pw1_bytes<S>(TY));
   static constexpr uint32_t BAR_BYTES = 128;
   // dynamic shared memory: barriers + rings + 128 B of alignment slack
   static constexpr uint32_t SMEM = BAR_BYTES + NSS * ST_SLOT + (NPW > 0 ? NPS * PW_SLOT : 0) + 128;
 };
 
-template <class S, class C, int R, int KIND, int TY>
-__global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ TmaMaps maps, const StageArgs a) {
-  using T = StageTraits<KIND>;
-  using LY = TmaLayout<S, R, KIND, TY>;
-  constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w();
-  constexpr int NT = TX * TY, NSS = LY::NSS, NPS = LY::NPS, NPW = T::NPW;
+// Ring state of one CTA.  Loads are numbered globally over the CTA's
+// lifetime (a persistent CTA processes many work items): load G sits in
+// slot G % NSS and completes phase G / NSS of that slot's barrier.
+struct TmaRing {
+  uint64_t* sbar;
+  uint64_t* pbar;
+  unsigned char* sring;
+  unsigned char* pring;
+  int sbase, pbase;  // loads issued for earlier work items
+};
 
-  extern __shared__ unsigned char smem_raw[];
-  __shared__ int s_abort;
+template <class LY>
+__device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* s_abort) {
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-  uint64_t* sbar = (uint64_t*)smem;   // NSS stencil barriers
-  uint64_t* pbar = sbar + NSS;        // NPS point-wise barriers
-  unsigned char* sring = smem + LY::BAR_BYTES;
-  unsigned char* pring = sring + NSS * LY::ST_SLOT;
-
-  const Geom& g = a.g;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i = blockIdx.x * TX + tx;
-  const int j = blockIdx.y * TY + ty;
-  const int kb = blockIdx.z * a.zc;
-  const int ke = min(kb + a.zc, g.nz);
-  const int M = ke - kb;          // planes updated by this CTA
-  const int L = M + 2 * R;        // stencil planes read: kb-R .. ke+R-1
-  const bool active = (i < g.nx) && (j < g.ny);
-  const long long col = (long long)(j + 2) * g.px + g.xoff + i;
-
-  // box origins in the padded tensor, in scalars (x) / rows (y) / planes (z)
-  const int cxs = 2 * (g.xoff + blockIdx.x * TX - HX);
-  const int cys = blockIdx.y * TY - R + 2;
-  const int cxp = 2 * (g.xoff + blockIdx.x * TX);
-  const int cyp = blockIdx.y * TY + 2;
-
-  if (tid == 0) {
-    s_abort = 0;
-    for (int s = 0; s < NSS; ++s) mbar_init(&sbar[s], 1);
-    for (int s = 0; s < NPS; ++s) mbar_init(&pbar[s], 1);
+  TmaRing rg;
+  rg.sbar = (uint64_t*)smem;
+  rg.pbar = rg.sbar + LY::NSS;
+  rg.sring = smem + LY::BAR_BYTES;
+  rg.pring = rg.sring + LY::NSS * LY::ST_SLOT;
+  rg.sbase = rg.pbase = 0;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    *s_abort = 0;
+    for (int s = 0; s < LY::NSS; ++s) mbar_init(&rg.sbar[s], 1);
+    for (int s = 0; s < LY::NPS; ++s) mbar_init(&rg.pbar[s], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  return rg;
+}
+
+// One work item: the 32 x TY tile (bx, by) of planes [bz*zc, bz*zc+zc) of one
+// solve.  Returns false when a bounded wait expired (the caller must stop;
+// the copies this item issued have been drained and a.status set).
+template <class S, class C, int R, int KIND, int TY, class LY>
+__device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
+                                         TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
+                                         double& r_err) {
+  using T = StageTraits<KIND>;
+  constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w();
+  constexpr int NSS = LY::NSS, NPS = LY::NPS, NPW = T::NPW;
+  constexpr uint32_t ST_BYTES = tma_st_bytes<S>(R, TY), PW1 = tma_pw1_bytes<S>(TY);
+
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i = bx * TX + tx;
+  const int j = by * TY + ty;
+  const int kb = bz * a.zc;
+  const int ke = min(kb + a.zc, g.nz);
+  const int M = ke - kb;    // planes updated by this item
+  const int L = M + 2 * R;  // stencil planes read: kb-R .. ke+R-1
+  const bool active = (i < g.nx) && (j < g.ny);
+  const long long col = (long long)(j + 2) * g.px + g.xoff + i;
+  const int SB = rg.sbase, PB = rg.pbase;
+
+  // box origins in the padded tensor, in scalars (x) / rows (y) / planes (z)
+  const int cxs = 2 * (g.xoff + bx * TX - HX);
+  const int cys = by * TY - R + 2;
+  const int cxp = 2 * (g.xoff + bx * TX);
+  const int cyp = by * TY + 2;
 
   int issued_s = 0, issued_p = 0;  // meaningful in thread 0 only
   auto issue_stencil = [&](int l) {
-    const int s = l % NSS;
-    mbar_arrive_expect_tx(&sbar[s], LY::ST_BYTES);
-    tma_load_3d(sring + s * LY::ST_SLOT, &maps.in, &sbar[s], cxs, cys, kb - R + l + 2);
+    const int G = SB + l, s = G % NSS;
+    mbar_arrive_expect_tx(&rg.sbar[s], ST_BYTES);
+    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, kb - R + l + 2);
     issued_s = l + 1;
   };
   auto issue_pw = [&](int m) {
     if constexpr (NPW > 0) {
-      const int s = m % NPS;
-      mbar_arrive_expect_tx(&pbar[s], NPW * LY::PW1_BYTES);
+      const int G = PB + m, s = G % NPS;
+      mbar_arrive_expect_tx(&rg.pbar[s], NPW * PW1);
 #pragma unroll
       for (int f = 0; f < NPW; ++f)
-        tma_load_3d(pring + s * LY::PW_SLOT + f * LY::PW1_BYTES, &maps.pw[f], &pbar[s], cxp, cyp, kb + m + 2);
+        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, kb + m + 2);
       issued_p = m + 1;
     }
   };
-  // on a timed-out wait: flag the error, let every copy this CTA issued land
+  auto swait = [&](int l) { return mbar_wait_bounded(&rg.sbar[(SB + l) % NSS], ((SB + l) / NSS) & 1); };
+  auto pwait = [&](int m) { return mbar_wait_bounded(&rg.pbar[(PB + m) % NPS], ((PB + m) / NPS) & 1); };
+  // on a timed-out wait: flag the error, let every copy this item issued land
   // (bounded), then leave
   auto drain = [&](int waited_s, int waited_p) {
     if (tid == 0) {
       atomicExch(a.status, 1);
-      for (int l = waited_s; l < issued_s; ++l) mbar_wait_bounded(&sbar[l % NSS], (l / NSS) & 1);
-      for (int m = waited_p; m < issued_p; ++m) mbar_wait_bounded(&pbar[m % NPS], (m / NPS) & 1);
+      for (int l = waited_s; l < issued_s; ++l) swait(l);
+      for (int m = waited_p; m < issued_p; ++m) pwait(m);
     }
     __syncthreads();
   };
@@ -174,18 +205,19 @@ __global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ T
   }
 
   const int cofs = (ty + R) * TW + tx + HX;  // this thread's centre in a stencil tile
+  auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
   S q[2 * R + 1];
   bool ok = true;
 #pragma unroll
   for (int l = 0; l < 2 * R; ++l) {
-    ok &= mbar_wait_bounded(&sbar[l % NSS], (l / NSS) & 1);
-    q[l] = ((const S*)(sring + (l % NSS) * LY::ST_SLOT))[cofs];
+    ok &= swait(l);
+    q[l] = stile(l)[cofs];
   }
-  if (!ok) s_abort = 1;
+  if (!ok) *s_abort = 1;
   __syncthreads();
-  if (s_abort) {
-    drain(2 * R, 0);
-    return;
+  if (*s_abort) {
+    drain(0, 0);
+    return false;
   }
   if (tid == 0) {
     fence_proxy_async();
@@ -194,22 +226,27 @@ __global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ T
   }
 
   const ColumnConsts cc = column_consts(a, i, j, R, active);
-  double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+  // ring cursors (slot, phase parity) of the lead plane, the centre plane
+  // and the point-wise plane, advanced incrementally
+  int sl_s = (SB + 2 * R) % NSS, sl_p = ((SB + 2 * R) / NSS) & 1;
+  int sc_s = (SB + R) % NSS;
+  int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
+  long long o = (long long)(kb + 2) * g.pz + col;  // element offset of (i, j, k)
 
   for (int m = 0; m < M; ++m) {
     const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
-    bool okw = mbar_wait_bounded(&sbar[ll % NSS], (ll / NSS) & 1);
-    q[2 * R] = ((const S*)(sring + (ll % NSS) * LY::ST_SLOT))[cofs];
+    bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
+    q[2 * R] = ((const S*)(rg.sring + sl_s * LY::ST_SLOT))[cofs];
     const S* pws = nullptr;
     if constexpr (NPW > 0) {
-      okw &= mbar_wait_bounded(&pbar[m % NPS], (m / NPS) & 1);
-      pws = (const S*)(pring + (m % NPS) * LY::PW_SLOT);
+      okw &= mbar_wait_bounded(&rg.pbar[pw_s], pw_p);
+      pws = (const S*)(rg.pring + pw_s * LY::PW_SLOT);
     }
-    if (!okw) s_abort = 1;
+    if (!okw) *s_abort = 1;
 
     if (active && okw) {
-      const S* tile = (const S*)(sring + (lc % NSS) * LY::ST_SLOT);
+      const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
       Nb<C> n;
       n.c0 = to_c<C>(q[R]);
       n.xm1 = to_c<C>(tile[cofs - 1]);
@@ -231,15 +268,20 @@ __global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ T
       S pv[NPW > 0 ? NPW : 1];
 #pragma unroll
       for (int f = 0; f < NPW; ++f) pv[f] = pws[f * (TX * TY) + tid];
-      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, col, cc, r_norm, r_en, r_err);
+      const int gz = (k <= R || k >= g.nz - 1 - R) ? ghost_pos(k, g.nz, R, a.bcs) : NOGHOST;
+      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, o, gz, cc, r_norm, r_en, r_err);
     }
 #pragma unroll
     for (int d = 0; d < 2 * R; ++d) q[d] = q[d + 1];
+    o += g.pz;
+    if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
+    if (++sc_s == NSS) sc_s = 0;
+    if (++pw_s == NPS) { pw_s = 0; pw_p ^= 1; }
 
     __syncthreads();  // every thread is done with stencil slot lc and point-wise slot m
-    if (s_abort) {
-      drain(ll + 1, m + 1);
-      return;
+    if (*s_abort) {
+      drain(ll, m);
+      return false;
     }
     if (tid == 0) {
       fence_proxy_async();
@@ -247,8 +289,70 @@ __global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ T
       if (m + NPS < M) issue_pw(m + NPS);
     }
   }
+  rg.sbase = SB + L;
+  rg.pbase = PB + (NPW > 0 ? M : 0);
+  return true;
+}
 
-  if (a.partials) block_reduce_store<NT>(r_norm, r_en, r_err, a.partials);
+// Single-solve stage kernel: one work item per CTA (grid = tiles x z-chunks).
+template <class S, class C, int R, int KIND, int TY>
+__global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ TmaMaps maps, const StageArgs a) {
+  using LY = TmaLayout<S, R, StageTraits<KIND>::NPW, TY>;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ int s_abort;
+  TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
+  double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+  if (!tma_item<S, C, R, KIND, TY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm, r_en,
+                                       r_err))
+    return;
+  if (a.partials) block_reduce_store<32 * TY>(r_norm, r_en, r_err, a.partials);
+}
+
+// ---------------------------------------------------------------------------
+// Batched, persistent stage kernel: many independent solves (any sizes, BCs,
+// orders 2 and 4) advanced by one launch per stage.  Work item w = tile
+// (bx, by, bz) of solve items[w].solve; CTA b processes items b, b + grid,
+// b + 2 grid, ...  Per-solve stage arguments and tensor maps live in a
+// device table; each CTA copies the item's arguments to shared memory.
+// Reductions go to per-item partials, summed per solve by k_finalize_ranges
+// in a fixed order, so a solve's results do not depend on what else is in
+// the batch.
+// ---------------------------------------------------------------------------
+struct alignas(64) BatchStage {
+  TmaMaps maps;
+  StageArgs args;
+};
+
+struct BatchItem {
+  int solve, bx, by, bz;
+};
+
+template <class S, class C, int KIND, int TY>
+__global__ void __launch_bounds__(32 * TY) k_stage_batch(const BatchStage* __restrict__ tab,
+                                                         const BatchItem* __restrict__ items, int nitems,
+                                                         double* partials) {
+  using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ int s_abort;
+  __shared__ StageArgs sa;
+  TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+    const BatchItem it = items[w];
+    const BatchStage* bs = tab + it.solve;
+    __syncthreads();  // previous item is done with sa
+    if (tid == 0) sa = bs->args;
+    __syncthreads();
+    const int R = sa.R;
+    double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+    bool ok;
+    if (R == 1)
+      ok = tma_item<S, C, 1, KIND, TY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en, r_err);
+    else
+      ok = tma_item<S, C, 2, KIND, TY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en, r_err);
+    if (!ok) return;
+    if (partials) block_reduce_store_at<32 * TY>(r_norm, r_en, r_err, partials, w);
+  }
 }
 
 }  // namespace gpe

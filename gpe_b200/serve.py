@@ -1,0 +1,149 @@
+"""Serving loop: a stream of Gross-Pitaevskii solve requests served by one
+GPU with continuous batching.
+
+Requests arrive over time (Poisson), are admitted into a Pool as soon as
+their state fits in the HBM budget, join the running batch at the next chunk
+boundary, and leave with their final state when done.  Latency of a request
+= completion time - arrival time (host clock).  Nothing here waits for the
+batch to drain before admitting new work.
+"""
+from __future__ import annotations
+
+import time
+from concurrent.futures import Future, ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import ic
+from .pool import Pool
+from .solver import RunParams
+
+
+@dataclass
+class Request:
+    tag: int
+    arrival_s: float
+    params: RunParams
+    nsteps: int
+    ic_kind: str          # "ring" | "line" | "random_phase"
+    seed: int
+    ic_arg: float = 0.0   # ring radius / random-phase cutoff
+
+    @property
+    def sites(self) -> int:
+        p = self.params
+        return p.nx * p.ny * p.nz
+
+
+def initial_state(req: Request) -> np.ndarray:
+    """Per-request initial state from its seed (host side)."""
+    p = req.params
+    if req.ic_kind == "ring":
+        psi = ic.vortex_ring(p, "xy", r0=req.ic_arg)
+    elif req.ic_kind == "line":
+        psi = ic.vortex_line_pade(p, dir="z")
+        if p.omx or p.omy or p.omz:
+            psi = ic.fermi(p) * psi
+    else:
+        psi = ic.random_phase(p, seed=req.seed, kc=req.ic_arg)
+    return psi.astype(np.complex64) if p.storage == "c64" else psi
+
+
+def make_requests(n: int, rate_per_s: float = 20.0, seed: int = 2024,
+                  sizes=tuple(range(48, 257, 16)), steps=(200, 5000)) -> list[Request]:
+    """Synthetic request stream: Poisson arrivals; cubic sizes uniform in
+    `sizes`; steps uniform in [steps]; RK4 or RKF45; order 2 or 4; V = 0 or
+    an isotropic trap with omega uniform in [0.02, 0.1]; initial state ring /
+    line / random phase from a per-request seed; FP64 or FP32 storage."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate_per_s)
+        nn = int(rng.choice(sizes))
+        trap = bool(rng.integers(0, 2))
+        om = float(rng.uniform(0.02, 0.1)) if trap else 0.0
+        scheme = "rk4" if rng.integers(0, 2) == 0 else "rk45"
+        kind = ("ring", "line", "random_phase")[int(rng.integers(0, 3))]
+        if kind == "random_phase":
+            trap, om = False, 0.0
+        h = 0.25 * (nn - 1)  # dx = 0.5
+        mu = 1.0
+        if trap:
+            # Thomas-Fermi radius covers the box: mu = 1 + V at the corner
+            mu = 1.0 + 0.5 * om * om * 3 * h * h
+        rp = RunParams(nx=nn, ny=nn, nz=nn, xr=h, yr=h, zr=h, tau=0.01 if scheme == "rk4" else 0.005,
+                       scheme=scheme, eqn_to_solve=4, bcs=1 if kind == "random_phase" else 2,
+                       order=int(rng.choice([2, 4])), g=1.0, mu=mu, omx=om, omy=om, omz=om,
+                       storage="c128" if rng.integers(0, 2) == 0 else "c64")
+        arg = float(rng.uniform(2.0, 6.0)) if kind == "ring" else float(rng.uniform(1.0, 2.0))
+        out.append(Request(k, t, rp, int(rng.integers(steps[0], steps[1] + 1)), kind, int(rng.integers(1 << 30)),
+                           arg))
+    return out
+
+
+@dataclass
+class ServeReport:
+    latencies_s: dict = field(default_factory=dict)
+    site_updates: int = 0
+    wall_s: float = 0.0
+    max_active: int = 0
+    rejected_admissions: int = 0
+
+    def summary(self) -> dict:
+        lat = np.array(sorted(self.latencies_s.values()))
+        return {"requests": int(len(lat)), "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                "site_updates_per_s": self.site_updates / self.wall_s if self.wall_s else None,
+                "wall_s": self.wall_s, "max_active": self.max_active,
+                "deferred_admissions": self.rejected_admissions}
+
+
+def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime: bool = True,
+          prep_threads: int = 4) -> ServeReport:
+    """Run the request stream through one Pool.  With realtime=True a request
+    becomes visible at its arrival time on the host clock; every loop turn
+    admits what has arrived and fits, advances the batch by up to `chunk`
+    steps, and collects finished solves."""
+    pool = Pool(budget_bytes)
+    rep = ServeReport()
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    # initial states are prepared on host threads as requests arrive (numpy
+    # releases the GIL in its FFT and array kernels); a request is admitted
+    # once its state is ready and fits in the budget
+    prep = ThreadPoolExecutor(max_workers=prep_threads)
+    waiting: list[tuple[Request, Future]] = []
+    by_tag = {r.tag: r for r in requests}
+    t0 = time.perf_counter()
+    active = 0
+    nxt = 0
+    while nxt < len(pending) or waiting or active:
+        now = time.perf_counter() - t0
+        while nxt < len(pending) and (not realtime or pending[nxt].arrival_s <= now):
+            waiting.append((pending[nxt], prep.submit(initial_state, pending[nxt])))
+            nxt += 1
+        still = []
+        for req, fut in waiting:
+            if not fut.done():
+                still.append((req, fut))
+            elif pool.submit(req.params, fut.result(), req.nsteps, req.tag):
+                active += 1
+            else:
+                rep.rejected_admissions += 1
+                still.append((req, fut))
+        waiting = still
+        if active == 0:
+            time.sleep(0.002)
+            continue
+        rep.max_active = max(rep.max_active, active)
+        active = pool.step(chunk)
+        done_t = time.perf_counter() - t0
+        for r in pool.poll():
+            req = by_tag[r.tag]
+            rep.latencies_s[r.tag] = done_t - req.arrival_s
+            rep.site_updates += req.sites * r.steps
+    rep.wall_s = time.perf_counter() - t0
+    prep.shutdown()
+    pool.close()
+    return rep

@@ -50,6 +50,7 @@ class RunParams:
     gamma: float = 0.0
     storage: str = "c128"      # "c128" | "c64"
     compute: str = "auto"      # stencil compute type for c64 storage: "auto" | "f32" | "f64"
+    tile_zc: int = 0           # z planes per CTA work item (0 = library default; set by the autotuner)
     eps: float = 0.0
     safety: float = 0.0
     dt_decrease: float = 0.0
@@ -65,6 +66,7 @@ class RunParams:
         p.real_time = 1 if self.real_time else 0
         p.storage = {"c128": L.GPE_C128, "c64": L.GPE_C64}[self.storage]
         p.compute = {"auto": L.GPE_COMPUTE_AUTO, "f32": L.GPE_COMPUTE_F32, "f64": L.GPE_COMPUTE_F64}[self.compute]
+        p.tile_zc = int(self.tile_zc)
         for f in ("xr", "yr", "zr", "tau", "Urhs", "diss_amp", "scal", "g", "mu", "nn", "omx", "omy",
                   "omz", "gamma", "eps", "safety", "dt_decrease", "dt_increase"):
             setattr(p, f, float(getattr(self, f)))

@@ -69,6 +69,8 @@ typedef struct {
   int32_t real_time;       /* 1: dt = tau, 0: dt = -i tau (src/gpe.f90:78-82) */
   int32_t storage;         /* GPE_C128 | GPE_C64 device storage of psi/stages */
   int32_t compute;         /* GPE_COMPUTE_* (GPE_C64 storage only)            */
+  int32_t tile_zc;         /* z planes per CTA work item; 0 = library default  */
+  int32_t reserved;        /* must be 0                                        */
   double xr, yr, zr;       /* half box lengths                                 */
   double tau;              /* |dt| (run.in tau)                                */
   double Urhs, diss_amp, scal, g, mu, nn, omx, omy, omz;
@@ -166,6 +168,44 @@ int gpe_profile(gpe_handle* h, int32_t enable);
  * the kind's algorithmic HBM bytes per grid site per launch (one read of
  * each input field, one write of each output field). */
 int gpe_profile_get(gpe_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes_per_site);
+
+/*
+ * Batched solves and serving (no reference counterpart: the reference runs
+ * exactly one solve per MPI job).  A pool owns one device arena of
+ * budget_bytes.  gpe_pool_submit admits a solve if its state fits in the
+ * free part of the arena (else GPE_ERR_NOMEM_BUDGET: retry after results
+ * have been polled); the solve joins the running batch at the next
+ * gpe_pool_step.  gpe_pool_step advances every active solve by up to
+ * max_steps steps with one persistent launch per Runge-Kutta stage per
+ * (precision, scheme) class over all their tiles, then retires the solves
+ * that reached their step count: the final state is copied to the caller's
+ * psi_out buffer (same element type as the solve's storage) and a
+ * gpe_result is queued for gpe_pool_poll.  Supported schemes: RK4 and RK45.
+ * Each solve evolves exactly as it would alone (same arithmetic per site,
+ * per-solve reductions in a fixed order).
+ */
+typedef struct gpe_pool gpe_pool;
+
+typedef struct {
+  uint64_t tag;
+  int32_t status;          /* GPE_OK or the error that stopped this solve      */
+  int32_t reserved;
+  int64_t steps, rejected; /* accepted steps; RKF45 rejected attempts          */
+  double t, im_t, dt_re, dt_im;
+  double norm;             /* get_norm of the final state                       */
+  double submit_s, start_s, finish_s; /* host seconds since gpe_pool_create   */
+} gpe_result;
+
+int gpe_pool_create(int64_t budget_bytes, gpe_pool** out);
+int gpe_pool_submit(gpe_pool* pool, const gpe_params* p, const void* psi0, int32_t dtype, int64_t nsteps,
+                    uint64_t tag, void* psi_out);
+int gpe_pool_step(gpe_pool* pool, int64_t max_steps, int32_t* n_active);
+int gpe_pool_poll(gpe_pool* pool, gpe_result* out, int32_t max, int32_t* n_out);
+int64_t gpe_pool_free_bytes(const gpe_pool* pool);
+/* Arena bytes one solve with these parameters needs (state + tables). */
+int64_t gpe_pool_solve_bytes(const gpe_params* p);
+const char* gpe_pool_last_error(const gpe_pool* pool);
+void gpe_pool_destroy(gpe_pool* pool);
 
 /* Bytes of device memory a solve with these parameters allocates. */
 int64_t gpe_state_bytes(const gpe_params* p);
