@@ -77,6 +77,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// Order a tensor map that sits in global memory (written by the host
+// between launches) before the async proxy reads it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((uint64_t)map) : "memory");
+}
+
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
                                             int c2) {
   asm volatile(
@@ -341,7 +347,11 @@ __global__ void __launch_bounds__(32 * TY) k_stage_batch(const BatchStage* __res
     const BatchItem it = items[w];
     const BatchStage* bs = tab + it.solve;
     __syncthreads();  // previous item is done with sa
-    if (tid == 0) sa = bs->args;
+    if (tid == 0) {
+      sa = bs->args;
+      tensormap_acquire(&bs->maps.in);
+      for (int f = 0; f < StageTraits<KIND>::NPW; ++f) tensormap_acquire(&bs->maps.pw[f]);
+    }
     __syncthreads();
     const int R = sa.R;
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
