@@ -5,7 +5,9 @@ a size is measured once per machine.
 
 The x-y tile is fixed by the TMA box (32 x 8 sites); tile_zc trades the
 z-halo re-read (2R planes per item) against the number of items, which
-matters most for the small and uneven grids of a batched workload.
+matters most for the small and uneven grids of a batched workload.  Shapes
+are timed in that setting: a pool holding enough copies of the solve to
+fill the GPU.
 """
 from __future__ import annotations
 
@@ -15,10 +17,10 @@ from pathlib import Path
 
 import numpy as np
 
-from .solver import RunParams, Solver
+from .solver import RunParams
 
 CACHE = Path(os.environ.get("GPE_TUNE_CACHE", Path(__file__).resolve().parent / "tune_cache.json"))
-CANDIDATES = (4, 8, 16, 32)
+CANDIDATES = (4, 8, 16, 32, 64)
 
 
 def _key(n: int, order: int, storage: str) -> str:
@@ -36,22 +38,26 @@ def save_cache(c: dict) -> None:
     CACHE.write_text(json.dumps(c, indent=1, sort_keys=True) + "\n")
 
 
-def time_rk4(rp: RunParams, steps: int = 20) -> float:
-    """Seconds per RK4 step of one solve (CUDA events on its stream)."""
-    import torch
+def time_rk4(rp: RunParams, steps: int = 20, target_sites: int = 32 << 20) -> float:
+    """Seconds per site per RK4 step when the GPU is kept busy with copies of
+    this solve in one pool (the batched setting the tuned shape is used in)."""
+    import time
 
-    s = Solver(rp)
-    s.set_state(np.ones((rp.nz, rp.ny, rp.nx), np.complex128))
-    st = torch.cuda.ExternalStream(s.stream())
-    s.solver(3)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    s.solver(steps, wait=False)
-    e1.record(st)
-    s.sync()
-    t = e0.elapsed_time(e1) * 1e-3 / steps
-    s.close()
-    return t
+    from .pool import Pool
+
+    n_sites = rp.nx * rp.ny * rp.nz
+    copies = max(1, min(64, -(-target_sites // n_sites)))
+    pool = Pool(Pool.solve_bytes(rp) * copies + (64 << 20))
+    psi = np.ones((rp.nz, rp.ny, rp.nx), np.complex64 if rp.storage == "c64" else np.complex128)
+    for c in range(copies):
+        pool.submit(rp, psi, steps + 4, c)
+    pool.step(3)  # joins the batch, captures the step graph
+    t0 = time.perf_counter()
+    pool.step(steps)
+    t = time.perf_counter() - t0
+    pool.run_all()
+    pool.close()
+    return t / (steps * copies * n_sites)
 
 
 def best_zc(n: int, order: int, storage: str, cache: dict | None = None) -> int:
@@ -64,7 +70,7 @@ def best_zc(n: int, order: int, storage: str, cache: dict | None = None) -> int:
         base = RunParams(nx=n, ny=n, nz=n, xr=h, yr=h, zr=h, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=1,
                          order=order, storage=storage)
         times = {zc: time_rk4(base.replace(tile_zc=zc)) for zc in CANDIDATES if zc <= n}
-        cache[k] = {"zc": min(times, key=times.get), "s_per_step": times}
+        cache[k] = {"zc": min(times, key=times.get), "s_per_site_step": times}
         if own:
             save_cache(cache)
     return int(cache[k]["zc"])

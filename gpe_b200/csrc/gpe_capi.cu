@@ -79,6 +79,7 @@ struct gpe_handle {
   long long prof_n[K_NUM] = {0};
   // kernel variant: true = TMA plane pipeline (k_stage_tma), false = k_stage
   bool use_tma = true;
+  int tma_ty = 4;  // threads per CTA in y for the 32 x 8 tile: 4 = two rows per thread, 8 = one
   std::vector<CUtensorMap> map_halo, map_pw;  // per field
   int* status = nullptr;                      // device status word
 };
@@ -143,9 +144,9 @@ cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a_in) {
     m.pw[t] = h->map_pw[f];
   }
   switch (h->cmode) {
-    case CM_F64: return launch_stage_tma_f64(kind, h->R, 8, h->grid, h->st, m, a);
-    case CM_F32: return launch_stage_tma_f32(kind, h->R, 8, h->grid, h->st, m, a);
-    default: return launch_stage_tma_f32x(kind, h->R, 8, h->grid, h->st, m, a);
+    case CM_F64: return launch_stage_tma_f64(kind, h->R, h->tma_ty, h->grid, h->st, m, a);
+    case CM_F32: return launch_stage_tma_f32(kind, h->R, h->tma_ty, h->grid, h->st, m, a);
+    default: return launch_stage_tma_f32x(kind, h->R, h->tma_ty, h->grid, h->st, m, a);
   }
 }
 
@@ -499,6 +500,7 @@ int gpe_create(const gpe_params* p, gpe_handle** out) {
     cudaMemsetAsync(h->fields[f], 0, (size_t)h->nelem * h->esz, h->st);
   }
   if (const char* e = getenv("GPE_KERNEL")) h->use_tma = strcmp(e, "ldg") != 0;
+  if (const char* e = getenv("GPE_ROWS_PER_THREAD")) h->tma_ty = atoi(e) == 1 ? 8 : 4;
   if (h->use_tma) {
     h->map_halo.resize(nf);
     h->map_pw.resize(nf);

@@ -8,6 +8,9 @@
 
 namespace gpe {
 
+// rows of the 32 x 8 tile owned by each thread of the batched kernel
+constexpr int BATCH_PY = 2;
+
 template <class S, class C, int R, int TY>
 static cudaError_t launch_kind(int kind, dim3 grid, cudaStream_t st, const StageArgs& a) {
   const dim3 block(32, TY);
@@ -36,28 +39,28 @@ static cudaError_t launch_kind(int kind, dim3 grid, cudaStream_t st, const Stage
   return cudaGetLastError();
 }
 
-template <class S, class C, int R, int K, int TY>
+template <class S, class C, int R, int K, int TY, int PY>
 static cudaError_t launch_tma_one(dim3 grid, cudaStream_t st, const TmaMaps& m, const StageArgs& a) {
   using LY = TmaLayout<S, R, StageTraits<K>::NPW, TY>;
   static unsigned long long attr_set = 0;  // per instantiation, one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_tma<S, C, R, K, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)LY::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_stage_tma<S, C, R, K, TY, PY>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_set |= 1ULL << dev;
   }
-  k_stage_tma<S, C, R, K, TY><<<grid, dim3(32, TY), LY::SMEM, st>>>(m, a);
+  k_stage_tma<S, C, R, K, TY, PY><<<grid, dim3(32, TY / PY), LY::SMEM, st>>>(m, a);
   return cudaGetLastError();
 }
 
-template <class S, class C, int R, int TY>
+template <class S, class C, int R, int TY, int PY>
 static cudaError_t launch_tma_kind(int kind, dim3 grid, cudaStream_t st, const TmaMaps& m, const StageArgs& a) {
   switch (kind) {
 #define GPE_TCASE(K) \
   case K:            \
-    return launch_tma_one<S, C, R, K, TY>(grid, st, m, a);
+    return launch_tma_one<S, C, R, K, TY, PY>(grid, st, m, a);
     GPE_TCASE(K_EULER)
     GPE_TCASE(K_RK2_1)
     GPE_TCASE(K_RK2_2)
@@ -80,9 +83,15 @@ static cudaError_t launch_tma_kind(int kind, dim3 grid, cudaStream_t st, const T
 template <class S, class C>
 static cudaError_t launch_stage_tma_impl(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
                                          const StageArgs& a) {
-  if (ty != 8) return cudaErrorInvalidValue;
-  if (R == 1) return launch_tma_kind<S, C, 1, 8>(kind, grid, st, m, a);
-  if (R == 2) return launch_tma_kind<S, C, 2, 8>(kind, grid, st, m, a);
+  // ty selects the rows per thread: 8 = one row per thread (256 threads),
+  // 4 = two rows per thread (128 threads); the tile is 32 x 8 either way
+  if (ty == 8) {
+    if (R == 1) return launch_tma_kind<S, C, 1, 8, 1>(kind, grid, st, m, a);
+    if (R == 2) return launch_tma_kind<S, C, 2, 8, 1>(kind, grid, st, m, a);
+  } else if (ty == 4) {
+    if (R == 1) return launch_tma_kind<S, C, 1, 8, 2>(kind, grid, st, m, a);
+    if (R == 2) return launch_tma_kind<S, C, 2, 8, 2>(kind, grid, st, m, a);
+  }
   return cudaErrorInvalidValue;
 }
 
@@ -98,11 +107,13 @@ static cudaError_t batch_setup(int* occupancy) {
   if (dev >= 64) return cudaErrorInvalidDevice;
   if (!(done & (1ULL << dev))) {
     cudaError_t e =
-        cudaFuncSetAttribute(k_stage_batch<S, C, K, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
+        cudaFuncSetAttribute(k_stage_batch<S, C, K, 8, BATCH_PY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8>, 256, LY::SMEM);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8, BATCH_PY>, 256 / BATCH_PY,
+                                                      LY::SMEM);
     if (e != cudaSuccess) return e;
     occ[dev] = nsm * (per > 0 ? per : 1);
     done |= 1ULL << dev;
@@ -117,7 +128,7 @@ static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage*
   using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
   cudaError_t e = batch_setup<S, C, K>(nullptr);
   if (e != cudaSuccess) return e;
-  k_stage_batch<S, C, K, 8><<<grid, dim3(32, 8), LY::SMEM, st>>>(tab, items, nitems, partials);
+  k_stage_batch<S, C, K, 8, BATCH_PY><<<grid, dim3(32, 8 / BATCH_PY), LY::SMEM, st>>>(tab, items, nitems, partials);
   return cudaGetLastError();
 }
 

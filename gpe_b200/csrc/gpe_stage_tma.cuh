@@ -146,27 +146,28 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
 }
 
 // One work item: the 32 x TY tile (bx, by) of planes [bz*zc, bz*zc+zc) of one
-// solve.  Returns false when a bounded wait expired (the caller must stop;
-// the copies this item issued have been drained and a.status set).
-template <class S, class C, int R, int KIND, int TY, class LY>
+// solve, processed by 32 x (TY/PY) threads, each owning PY rows of the tile
+// (rows ty, ty + TY/PY, ...) so that the per-plane waits, barrier and ring
+// bookkeeping are shared by PY sites.  Returns false when a bounded wait
+// expired (the caller must stop; the copies this item issued have been
+// drained and a.status set).
+template <class S, class C, int R, int KIND, int TY, int PY, class LY>
 __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                          TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                          double& r_err) {
   using T = StageTraits<KIND>;
-  constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w();
+  constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w(), TYT = TY / PY;
   constexpr int NSS = LY::NSS, NPS = LY::NPS, NPW = T::NPW;
   constexpr uint32_t ST_BYTES = tma_st_bytes<S>(R, TY), PW1 = tma_pw1_bytes<S>(TY);
+  static_assert(TY % PY == 0, "PY must divide TY");
 
   const Geom& g = a.g;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int tx = threadIdx.x, tyt = threadIdx.y, tid = tyt * TX + tx;
   const int i = bx * TX + tx;
-  const int j = by * TY + ty;
   const int kb = bz * a.zc;
   const int ke = min(kb + a.zc, g.nz);
   const int M = ke - kb;    // planes updated by this item
   const int L = M + 2 * R;  // stencil planes read: kb-R .. ke+R-1
-  const bool active = (i < g.nx) && (j < g.ny);
-  const long long col = (long long)(j + 2) * g.px + g.xoff + i;
   const int SB = rg.sbase, PB = rg.pbase;
 
   // box origins in the padded tensor, in scalars (x) / rows (y) / planes (z)
@@ -210,14 +211,30 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     for (int m = 0; m < min(NPS, M); ++m) issue_pw(m);
   }
 
-  const int cofs = (ty + R) * TW + tx + HX;  // this thread's centre in a stencil tile
+  // per owned row: grid row, activity, centre offset in a stencil tile
+  int jr[PY], cofs[PY];
+  bool act[PY];
+  long long o[PY];  // element offset of (i, j, k)
+  ColumnConsts cc[PY];
+#pragma unroll
+  for (int r = 0; r < PY; ++r) {
+    const int ty = tyt + r * TYT;
+    jr[r] = by * TY + ty;
+    act[r] = (i < g.nx) && (jr[r] < g.ny);
+    cofs[r] = (ty + R) * TW + tx + HX;
+    o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i;
+    cc[r] = column_consts(a, i, jr[r], R, act[r]);
+  }
+
   auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
-  S q[2 * R + 1];
+  S q[PY][2 * R + 1];
   bool ok = true;
 #pragma unroll
   for (int l = 0; l < 2 * R; ++l) {
     ok &= swait(l);
-    q[l] = stile(l)[cofs];
+    const S* tl = stile(l);
+#pragma unroll
+    for (int r = 0; r < PY; ++r) q[r][l] = tl[cofs[r]];
   }
   if (!ok) *s_abort = 1;
   __syncthreads();
@@ -231,19 +248,21 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
       if (l + NSS < L) issue_stencil(l + NSS);
   }
 
-  const ColumnConsts cc = column_consts(a, i, j, R, active);
   // ring cursors (slot, phase parity) of the lead plane, the centre plane
   // and the point-wise plane, advanced incrementally
   int sl_s = (SB + 2 * R) % NSS, sl_p = ((SB + 2 * R) / NSS) & 1;
   int sc_s = (SB + R) % NSS;
   int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
-  long long o = (long long)(kb + 2) * g.pz + col;  // element offset of (i, j, k)
 
   for (int m = 0; m < M; ++m) {
     const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
     bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
-    q[2 * R] = ((const S*)(rg.sring + sl_s * LY::ST_SLOT))[cofs];
+    {
+      const S* tl = (const S*)(rg.sring + sl_s * LY::ST_SLOT);
+#pragma unroll
+      for (int r = 0; r < PY; ++r) q[r][2 * R] = tl[cofs[r]];
+    }
     const S* pws = nullptr;
     if constexpr (NPW > 0) {
       okw &= mbar_wait_bounded(&rg.pbar[pw_s], pw_p);
@@ -251,35 +270,44 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     }
     if (!okw) *s_abort = 1;
 
-    if (active && okw) {
+    if (okw) {
       const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
-      Nb<C> n;
-      n.c0 = to_c<C>(q[R]);
-      n.xm1 = to_c<C>(tile[cofs - 1]);
-      n.xp1 = to_c<C>(tile[cofs + 1]);
-      n.ym1 = to_c<C>(tile[cofs - TW]);
-      n.yp1 = to_c<C>(tile[cofs + TW]);
-      n.zm1 = to_c<C>(q[R - 1]);
-      n.zp1 = to_c<C>(q[R + 1]);
-      if constexpr (R == 2) {
-        n.xm2 = to_c<C>(tile[cofs - 2]);
-        n.xp2 = to_c<C>(tile[cofs + 2]);
-        n.ym2 = to_c<C>(tile[cofs - 2 * TW]);
-        n.yp2 = to_c<C>(tile[cofs + 2 * TW]);
-        n.zm2 = to_c<C>(q[0]);
-        n.zp2 = to_c<C>(q[4]);
-      } else {
-        n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
-      }
-      S pv[NPW > 0 ? NPW : 1];
-#pragma unroll
-      for (int f = 0; f < NPW; ++f) pv[f] = pws[f * (TX * TY) + tid];
       const int gz = (k <= R || k >= g.nz - 1 - R) ? ghost_pos(k, g.nz, R, a.bcs) : NOGHOST;
-      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, o, gz, cc, r_norm, r_en, r_err);
+#pragma unroll
+      for (int r = 0; r < PY; ++r) {
+        if (!act[r]) continue;
+        const int c0 = cofs[r];
+        Nb<C> n;
+        n.c0 = to_c<C>(q[r][R]);
+        n.xm1 = to_c<C>(tile[c0 - 1]);
+        n.xp1 = to_c<C>(tile[c0 + 1]);
+        n.ym1 = to_c<C>(tile[c0 - TW]);
+        n.yp1 = to_c<C>(tile[c0 + TW]);
+        n.zm1 = to_c<C>(q[r][R - 1]);
+        n.zp1 = to_c<C>(q[r][R + 1]);
+        if constexpr (R == 2) {
+          n.xm2 = to_c<C>(tile[c0 - 2]);
+          n.xp2 = to_c<C>(tile[c0 + 2]);
+          n.ym2 = to_c<C>(tile[c0 - 2 * TW]);
+          n.yp2 = to_c<C>(tile[c0 + 2 * TW]);
+          n.zm2 = to_c<C>(q[r][0]);
+          n.zp2 = to_c<C>(q[r][4]);
+        } else {
+          n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
+        }
+        S pv[NPW > 0 ? NPW : 1];
+        const int pofs = (tyt + r * TYT) * TX + tx;
+#pragma unroll
+        for (int f = 0; f < NPW; ++f) pv[f] = pws[f * (TX * TY) + pofs];
+        site_stage<S, C, R, KIND>(a, n, pv, i, jr[r], k, o[r], gz, cc[r], r_norm, r_en, r_err);
+      }
     }
 #pragma unroll
-    for (int d = 0; d < 2 * R; ++d) q[d] = q[d + 1];
-    o += g.pz;
+    for (int r = 0; r < PY; ++r) {
+#pragma unroll
+      for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
+      o[r] += g.pz;
+    }
     if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
     if (++sc_s == NSS) sc_s = 0;
     if (++pw_s == NPS) { pw_s = 0; pw_p ^= 1; }
@@ -301,17 +329,18 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
 }
 
 // Single-solve stage kernel: one work item per CTA (grid = tiles x z-chunks).
-template <class S, class C, int R, int KIND, int TY>
-__global__ void __launch_bounds__(32 * TY) k_stage_tma(const __grid_constant__ TmaMaps maps, const StageArgs a) {
+template <class S, class C, int R, int KIND, int TY, int PY>
+__global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constant__ TmaMaps maps,
+                                                           const StageArgs a) {
   using LY = TmaLayout<S, R, StageTraits<KIND>::NPW, TY>;
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item<S, C, R, KIND, TY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm, r_en,
-                                       r_err))
+  if (!tma_item<S, C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+                                           r_en, r_err))
     return;
-  if (a.partials) block_reduce_store<32 * TY>(r_norm, r_en, r_err, a.partials);
+  if (a.partials) block_reduce_store<32 * TY / PY>(r_norm, r_en, r_err, a.partials);
 }
 
 // ---------------------------------------------------------------------------
@@ -333,8 +362,8 @@ struct BatchItem {
   int solve, bx, by, bz;
 };
 
-template <class S, class C, int KIND, int TY>
-__global__ void __launch_bounds__(32 * TY) k_stage_batch(const BatchStage* __restrict__ tab,
+template <class S, class C, int KIND, int TY, int PY>
+__global__ void __launch_bounds__(32 * TY / PY) k_stage_batch(const BatchStage* __restrict__ tab,
                                                          const BatchItem* __restrict__ items, int nitems,
                                                          double* partials) {
   using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
@@ -357,11 +386,13 @@ __global__ void __launch_bounds__(32 * TY) k_stage_batch(const BatchStage* __res
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;
     if (R == 1)
-      ok = tma_item<S, C, 1, KIND, TY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en, r_err);
+      ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                               r_err);
     else
-      ok = tma_item<S, C, 2, KIND, TY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en, r_err);
+      ok = tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                               r_err);
     if (!ok) return;
-    if (partials) block_reduce_store_at<32 * TY>(r_norm, r_en, r_err, partials, w);
+    if (partials) block_reduce_store_at<32 * TY / PY>(r_norm, r_en, r_err, partials, w);
   }
 }
 
