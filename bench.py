@@ -333,6 +333,8 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32-storage and RKF45 legs")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling target: set up the workload and run 2 RK4 steps, nothing else")
+    ap.add_argument("--storage", default="c128", choices=["c128", "c64"],
+                    help="storage of the --ncu-case / --quick workload")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
@@ -342,8 +344,8 @@ def main() -> int:
 
     from gpe_b200 import dist
 
-    torch.cuda.set_device(local)
-    pg = dist.init(backend="nccl", timeout_s=120)
+    torch.cuda.set_device(local % max(1, torch.cuda.device_count()))
+    pg = dist.init(backend=os.environ.get("GPE_DIST_BACKEND", "nccl"), timeout_s=120)
 
     from gpe_b200 import _lib as L
     from gpe_b200 import ic
@@ -352,6 +354,8 @@ def main() -> int:
     rp = RunParams(**WORKLOAD)
     n_sites = rp.nx * rp.ny * rp.nz
     psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
+    if args.ncu_case or args.quick:
+        rp = rp.replace(storage=args.storage, compute="f32" if args.storage == "c64" else "auto")
     s = Solver(rp)
     s.set_state(psi0)
     stream = torch.cuda.ExternalStream(s.stream())

@@ -53,6 +53,26 @@ class GpeStepInfo(C.Structure):
     ]
 
 
+GPE_IC_UNIFORM, GPE_IC_FERMI, GPE_IC_LINE, GPE_IC_RING, GPE_IC_LINE_PADE, GPE_IC_RANDOM_PHASE = range(6)
+
+
+class GpeRing(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double), ("r0", C.c_double),
+                ("amp", C.c_double), ("r1", C.c_double), ("dir", C.c_double), ("mm", C.c_int32),
+                ("kk", C.c_int32), ("plane", C.c_char * 4), ("reserved", C.c_int32)]
+
+
+class GpeLine(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double), ("amp1", C.c_double),
+                ("amp2", C.c_double), ("ll", C.c_double), ("sgn", C.c_double), ("imprint_phase", C.c_int32),
+                ("dir", C.c_char), ("reserved", C.c_char * 3)]
+
+
+class GpeIC(C.Structure):
+    _fields_ = [("nfactors", C.c_int32), ("factor", C.c_int32 * 4), ("reserved", C.c_int32),
+                ("ring", GpeRing), ("line", GpeLine), ("seed", C.c_uint64), ("kc", C.c_double)]
+
+
 class GpeResult(C.Structure):
     _fields_ = [
         ("tag", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_int32),
@@ -86,6 +106,9 @@ _PROTOS = {
     "gpe_pool_create": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
     "gpe_pool_submit": (C.c_int, [C.c_void_p, C.POINTER(GpeParams), C.c_void_p, C.c_int32, C.c_int64, C.c_uint64,
                                   C.c_void_p]),
+    "gpe_pool_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeParams), C.POINTER(GpeIC), C.c_int64, C.c_uint64,
+                                     C.c_void_p]),
+    "gpe_set_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeIC)]),
     "gpe_pool_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
     "gpe_pool_poll": (C.c_int, [C.c_void_p, C.POINTER(GpeResult), C.c_int32, C.POINTER(C.c_int32)]),
     "gpe_pool_free_bytes": (C.c_int64, [C.c_void_p]),

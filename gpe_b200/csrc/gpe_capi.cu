@@ -21,6 +21,7 @@
 #include "gpe_device.cuh"
 #include "gpe_stage_tma.cuh"
 #include "gpe_common.h"
+#include "gpe_ic.h"
 
 namespace gpe {
 cudaError_t launch_stage_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
@@ -696,6 +697,19 @@ int gpe_renormalise(gpe_handle* h, double norm) {
   if (h->esz == 16) k_scale<double2><<<148 * 8, 256, 0, h->st>>>((double2*)h->fields[h->cur], h->nelem, a, b);
   else k_scale<float2><<<148 * 8, 256, 0, h->st>>>((float2*)h->fields[h->cur], h->nelem, a, b);
   CU(h, cudaGetLastError());
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_set_ic(gpe_handle* h, const gpe_ic* ic) {
+  if (!h) return GPE_ERR_BADARG;
+  std::string why;
+  if (int rc = ic_validate(ic, why)) return fail(h, rc, why);
+  CU(h, cudaSetDevice(h->dev));
+  const size_t wb = ic_work_bytes(h->p, *ic);
+  if (wb)
+    if (int rc = ensure_staging(h, wb)) return rc;
+  CU(h, ic_generate(h->p, h->g, h->esz, h->R, *ic, h->fields[h->cur], h->staging, h->staging_bytes, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   return GPE_OK;
 }

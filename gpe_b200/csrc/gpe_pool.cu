@@ -25,6 +25,7 @@
 #include "../../include/gpe_cuda.h"
 #include "gpe_aux.cuh"
 #include "gpe_common.h"
+#include "gpe_ic.h"
 
 namespace gpe {
 cudaError_t launch_batch_f64(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
@@ -549,15 +550,18 @@ int64_t gpe_pool_solve_bytes(const gpe_params* p) {
   return (int64_t)(fb * scheme_fields(p->scheme) + Arena::round(tables_bytes(*p)));
 }
 
-int gpe_pool_submit(gpe_pool* P, const gpe_params* prm, const void* psi0, int32_t dtype, int64_t nsteps,
-                    uint64_t tag, void* psi_out) {
-  if (!P || !prm || !psi0 || !psi_out || nsteps < 0) return pfail(P, GPE_ERR_BADARG, "null argument");
+static int pool_submit_impl(gpe_pool* P, const gpe_params* prm, const void* psi0, int32_t dtype,
+                            const gpe_ic* icspec, int64_t nsteps, uint64_t tag, void* psi_out) {
+  if (!P || !prm || !psi_out || nsteps < 0 || (!psi0 && !icspec)) return pfail(P, GPE_ERR_BADARG, "null argument");
   std::string why;
   if (int rc = validate_params(prm, why)) return pfail(P, rc, why);
+  if (icspec)
+    if (int rc = ic_validate(icspec, why)) return pfail(P, rc, why);
   if (prm->scheme != GPE_RK4 && prm->scheme != GPE_RK45)
     return pfail(P, GPE_ERR_BADARG, "the pool runs RK4 and RK45 solves");
   const int want = prm->storage == GPE_C128 ? GPE_C128 : GPE_C64;
-  if (dtype != want) return pfail(P, GPE_ERR_BADARG, "psi0/psi_out element type must match the solve's storage");
+  if (psi0 && dtype != want)
+    return pfail(P, GPE_ERR_BADARG, "psi0/psi_out element type must match the solve's storage");
   PCU(P, cudaSetDevice(P->dev));
   Solve* s = new Solve();
   s->tag = tag;
@@ -597,7 +601,17 @@ int gpe_pool_submit(gpe_pool* P, const gpe_params* prm, const void* psi0, int32_
       cudaMemcpyAsync(s->tables, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, P->st) !=
           cudaSuccess)
     return bail(GPE_ERR_CUDA, "upload of tables failed");
-  if (int rc = upload_state(P, s, psi0, 0)) return bail(rc, P->err);
+  if (psi0) {
+    if (int rc = upload_state(P, s, psi0, 0)) return bail(rc, P->err);
+  } else {
+    // the other fields are free until the first step: the generator's
+    // scratch (spectrum + FFT) lives there
+    const size_t wb = ic_work_bytes(*prm, *icspec);
+    const size_t room = (size_t)(s->nf - 1) * s->field_bytes;
+    if (wb > room) return bail(GPE_ERR_BADARG, "initial-condition scratch does not fit in the solve's fields");
+    if (ic_generate(*prm, s->g, s->esz, s->R, *icspec, s->f[0], s->f[1], room, P->st) != cudaSuccess)
+      return bail(GPE_ERR_CUDA, "device initial condition failed");
+  }
   if (cudaStreamSynchronize(P->st) != cudaSuccess) return bail(GPE_ERR_CUDA, "state upload failed");
   if (prm->real_time) { s->dr = prm->tau; s->di = 0.0; }
   else { s->dr = 0.0; s->di = -prm->tau; }
@@ -608,6 +622,18 @@ int gpe_pool_submit(gpe_pool* P, const gpe_params* prm, const void* psi0, int32_
   s->t_submit = now_s(P->t0);
   P->pending.push_back(s);
   return GPE_OK;
+}
+
+int gpe_pool_submit(gpe_pool* P, const gpe_params* prm, const void* psi0, int32_t dtype, int64_t nsteps,
+                    uint64_t tag, void* psi_out) {
+  if (!psi0) return pfail(P, GPE_ERR_BADARG, "null psi0");
+  return pool_submit_impl(P, prm, psi0, dtype, nullptr, nsteps, tag, psi_out);
+}
+
+int gpe_pool_submit_ic(gpe_pool* P, const gpe_params* prm, const gpe_ic* ic, int64_t nsteps, uint64_t tag,
+                       void* psi_out) {
+  if (!ic) return pfail(P, GPE_ERR_BADARG, "null initial-condition spec");
+  return pool_submit_impl(P, prm, nullptr, 0, ic, nsteps, tag, psi_out);
 }
 
 int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {

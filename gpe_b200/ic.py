@@ -155,3 +155,32 @@ def random_phase(p, seed: int = 1234, kc: float = 1.5):
     psi = np.fft.ifftn(spec)
     psi *= 1.0 / np.sqrt(np.mean(np.abs(psi) ** 2))
     return np.ascontiguousarray(psi, dtype=np.complex128)
+
+
+# ---------------------------------------------------------------------------
+# Device-side initial conditions: specs for gpe_set_ic / gpe_pool_submit_ic
+
+
+def device_spec(*factors, ring=None, line=None, seed: int = 1234, kc: float = 1.5):
+    """Build a gpe_ic spec: the product of the named factors ("uniform",
+    "fermi", "line", "ring", "line_pade", "random_phase").  ring / line are
+    dicts with the fields of ring_param / line_param (src/parameters.in)."""
+    from . import _lib as L
+
+    codes = {"uniform": L.GPE_IC_UNIFORM, "fermi": L.GPE_IC_FERMI, "line": L.GPE_IC_LINE,
+             "ring": L.GPE_IC_RING, "line_pade": L.GPE_IC_LINE_PADE, "random_phase": L.GPE_IC_RANDOM_PHASE}
+    spec = L.GpeIC()
+    spec.nfactors = len(factors)
+    for q, f in enumerate(factors):
+        spec.factor[q] = codes[f]
+    r = dict(plane="xy", x0=0.0, y0=0.0, z0=0.0, r0=4.0, amp=0.0, mm=0, r1=0.0, kk=0, dir=1.0)
+    r.update(ring or {})
+    for k, v in r.items():
+        setattr(spec.ring, k, v.encode() if k == "plane" else v)
+    ln = dict(x0=0.0, y0=0.0, z0=0.0, amp1=0.0, amp2=0.0, ll=0.0, sgn=1.0, dir="z", imprint_phase=0)
+    ln.update(line or {})
+    for k, v in ln.items():
+        setattr(spec.line, k, v.encode() if k == "dir" else (int(v) if k == "imprint_phase" else v))
+    spec.seed = int(seed)
+    spec.kc = float(kc)
+    return spec

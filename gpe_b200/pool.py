@@ -90,6 +90,20 @@ class Pool:
         self._out[int(tag)] = out
         return True
 
+    def submit_ic(self, params: RunParams, spec, nsteps: int, tag: int) -> bool:
+        """Admit a solve whose initial state is generated on the device."""
+        dt = np.complex64 if params.storage == "c64" else np.complex128
+        out = np.empty((params.nz, params.ny, params.nx), dtype=dt)
+        cp = params.to_c()
+        rc = self.lib.gpe_pool_submit_ic(self.h, C.byref(cp), C.byref(spec), int(nsteps), int(tag),
+                                         out.ctypes.data)
+        if rc == L.GPE_ERR_NOMEM_BUDGET:
+            return False
+        if rc != L.GPE_OK:
+            raise self._err(rc)
+        self._out[int(tag)] = out
+        return True
+
     def step(self, max_steps: int) -> int:
         n = C.c_int32()
         rc = self.lib.gpe_pool_step(self.h, int(max_steps), C.byref(n))

@@ -142,6 +142,10 @@ class Solver:
         _check(self.lib, self.h, self.lib.gpe_get_state(self.h, out.ctypes.data, code))
         return out
 
+    def set_ic(self, spec) -> None:
+        """Generate the initial state on the device (see ic.device_spec)."""
+        _check(self.lib, self.h, self.lib.gpe_set_ic(self.h, C.byref(spec)))
+
     # -- stepping -----------------------------------------------------------
     def solver(self, nsteps: int = 1, want_norm: bool = False, want_energy: bool = False,
                wait: bool = True) -> L.GpeStepInfo:

@@ -147,6 +147,46 @@ int gpe_get_grid(const gpe_handle* h, double* x, double* y, double* z, double* d
 /* The CUDA stream (cudaStream_t) all of the handle's work runs on. */
 int gpe_get_stream(const gpe_handle* h, void** stream);
 
+/*
+ * Initial conditions generated on the device (replaces the host-side
+ * ics()/ic.in evaluation, src/ic.f90:84-113, for the products ic.in can
+ * express).  The state is the product of up to four factors, each one of:
+ */
+#define GPE_IC_UNIFORM 0      /* 1                                                 */
+#define GPE_IC_FERMI 1        /* fermi(): sqrt(max(mu - V, 0)/g), src/ic.f90:278  */
+#define GPE_IC_LINE 2         /* vortex_line(vl), core 1-exp(-0.7 r^1.15), :332   */
+#define GPE_IC_RING 3         /* vortex_ring(vr), Pade core, src/ic.f90:357       */
+#define GPE_IC_LINE_PADE 4    /* straight line with the Pade core r*get_rr(r)     */
+#define GPE_IC_RANDOM_PHASE 5 /* seeded spectrum |k| < kc, inverse FFT, mean
+                                 density 1 (must be the only factor)               */
+
+typedef struct {              /* ring_param, src/parameters.in:54-68 */
+  double x0, y0, z0, r0, amp, r1, dir;
+  int32_t mm, kk;
+  char plane[4];              /* "xy", "xz" or "yz" */
+  int32_t reserved;
+} gpe_ring;
+
+typedef struct {              /* line_param, src/parameters.in:32-43 */
+  double x0, y0, z0, amp1, amp2, ll, sgn;
+  int32_t imprint_phase;
+  char dir;                   /* 'x', 'y' or 'z' */
+  char reserved[3];
+} gpe_line;
+
+typedef struct {
+  int32_t nfactors;           /* 1..4 */
+  int32_t factor[4];          /* GPE_IC_* */
+  int32_t reserved;
+  gpe_ring ring;
+  gpe_line line;
+  uint64_t seed;              /* GPE_IC_RANDOM_PHASE */
+  double kc;                  /* GPE_IC_RANDOM_PHASE cutoff |k| < kc */
+} gpe_ic;
+
+/* Set the handle's state to the initial condition (no host array). */
+int gpe_set_ic(gpe_handle* h, const gpe_ic* ic);
+
 /* Stage-kernel kinds reported by gpe_profile_get (one fused kernel each). */
 #define GPE_KIND_EULER 0
 #define GPE_KIND_RK2_1 1
@@ -199,6 +239,9 @@ typedef struct {
 int gpe_pool_create(int64_t budget_bytes, gpe_pool** out);
 int gpe_pool_submit(gpe_pool* pool, const gpe_params* p, const void* psi0, int32_t dtype, int64_t nsteps,
                     uint64_t tag, void* psi_out);
+/* Same, with the initial state generated on the device from an IC spec. */
+int gpe_pool_submit_ic(gpe_pool* pool, const gpe_params* p, const gpe_ic* ic, int64_t nsteps, uint64_t tag,
+                       void* psi_out);
 int gpe_pool_step(gpe_pool* pool, int64_t max_steps, int32_t* n_active);
 int gpe_pool_poll(gpe_pool* pool, gpe_result* out, int32_t max, int32_t* n_out);
 int64_t gpe_pool_free_bytes(const gpe_pool* pool);
