@@ -73,6 +73,20 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+BIN = PKG / "bin"
+HOST_SRC = CSRC / "host" / "gpe_host.cpp"
+HOST = BIN / "gpe_host"
+
+
+def build_host(force: bool = False, verbose: bool = False) -> Path:
+    """The C++ driver that runs the reference's time loop over the C ABI."""
+    BIN.mkdir(exist_ok=True)
+    if force or not HOST.exists() or HOST.stat().st_mtime < max(HOST_SRC.stat().st_mtime, LIB.stat().st_mtime):
+        _run(["g++", "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), str(HOST_SRC), "-o", str(HOST),
+              "-L", str(LIBDIR), "-lgpe_cuda", "-Wl,-rpath,$ORIGIN/../lib"], verbose)
+    return HOST
+
+
 def build_oracle(verbose: bool = False) -> None:
     """The CPU oracle is test infrastructure; it has its own recipe."""
     _run(["make", "-s", "-C", str(ROOT / "oracle")], verbose)
@@ -82,7 +96,8 @@ def main(argv: list[str]) -> int:
     force = "--force" in argv
     verbose = "-v" in argv or "--verbose" in argv
     lib = build_library(force=force, verbose=verbose)
-    print(f"built {lib}")
+    host = build_host(force=force, verbose=verbose)
+    print(f"built {lib} and {host}")
     return 0
 
 

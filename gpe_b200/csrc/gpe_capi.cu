@@ -357,7 +357,10 @@ int rk45_step(gpe_handle* h, gpe_step_info* io, bool energy, bool norm) {
     const double e = pow(errmax, dtdec);
     const double tr = (safety * dr) * e, ti = (safety * di) * e;
     const double m = std::max(hypot(tr, ti), 0.1 * hypot(dr, di));
-    if (!p.real_time) { dr = 0.0; di = -m; }
+    // real time <=> dt on the real axis (src/solve.f90:197-201 tests the
+    // real_time flag; dt is (tau, 0) exactly when it is set, also after the
+    // imaginary-to-real switch of src/gpe.f90:264)
+    if (!(di == 0.0)) { dr = 0.0; di = -m; }
     else { dr = m; di = 0.0; }
   }
   double nr, ni;

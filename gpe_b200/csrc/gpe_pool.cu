@@ -476,7 +476,7 @@ int run_rk45(gpe_pool* P, int cm) {
         const double e = pow(errmax, dtdec);
         const double tr = (safety * s->dr) * e, ti = (safety * s->di) * e;
         const double mm = std::max(hypot(tr, ti), 0.1 * hypot(s->dr, s->di));
-        if (!p.real_time) { s->dr = 0.0; s->di = -mm; }
+        if (!(s->di == 0.0)) { s->dr = 0.0; s->di = -mm; }  // imaginary time: dt on the negative imaginary axis
         else { s->dr = mm; s->di = 0.0; }
         continue;
       }

@@ -1,0 +1,80 @@
+"""End-to-end runs of the C++ host driver on the GPU: the reference's input
+files in, the reference's output files out, state identical to the same
+solve through the Python interface and within 1e-12 of the CPU oracle;
+restart from end_state continues the run exactly."""
+from __future__ import annotations
+
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gpe_b200 import ic
+from gpe_b200.build import HOST
+from gpe_b200.solver import RunParams, Solver
+from oracle.pyoracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+INPUTS = Path(__file__).resolve().parent / "golden" / "inputs"
+RP = RunParams(nx=64, ny=64, nz=64, xr=15.75, yr=15.75, zr=15.75, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=2,
+               order=2, g=1.0, mu=1.0)
+
+
+def read_end_state(path: Path):
+    b = path.read_bytes()
+    nx, ny, nz, p = np.frombuffer(b[:16], dtype=np.int32)
+    t, im_t, dr, di = np.frombuffer(b[16:48], dtype=np.float64)
+    psi = np.frombuffer(b[48:], dtype=np.complex128).reshape(nz, ny, nx)
+    return int(p), t, im_t, complex(dr, di), psi
+
+
+def run(d):
+    r = subprocess.run([str(HOST), "--dir", str(d)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+def test_host_run_and_restart(gpu, tmp_path):
+    d = tmp_path / "run"
+    shutil.copytree(INPUTS / "ring64", d)
+    run(d)
+    p, t, im_t, dt, psi = read_end_state(d / "proc0000" / "end_state.dat")
+    assert p == 10 and t == pytest.approx(0.1, rel=1e-12) and im_t == 0.0 and dt == 0.01
+    assert not (d / "RUNNING").exists() and not (d / "ERROR").exists()
+    # same solve through the Python interface, device ring IC
+    s = Solver(RP)
+    s.set_ic(ic.device_spec("ring", ring=dict(plane="xy", r0=4.0)))
+    s.solver(10)
+    np.testing.assert_array_equal(psi, s.get_state())
+    # the CPU oracle from the host ring IC
+    ref = Oracle(RP).run(ic.vortex_ring(RP, "xy", r0=4.0), 10)
+    assert np.linalg.norm(psi - ref) / np.linalg.norm(ref) <= 1e-12
+    # time series: e17.9 records, energy every save_rate = 2 steps
+    e = (d / "energy.dat").read_text().splitlines()
+    nrm = (d / "norm.dat").read_text().splitlines()
+    # (how many records depends on the accumulated t, as in the reference's
+    # modulo(t+im_t, |dt|*save_rate) < |dt| test)
+    assert len(e) >= 2 and all(len(x) == 51 for x in e)
+    assert len(nrm) >= 2 and all(len(x) == 68 for x in nrm)
+    assert float(nrm[-1].split()[2]) == pytest.approx(s.get_norm(), rel=1e-12)
+    # restart from the end state for 10 more steps == 20 steps straight
+    shutil.copy(d / "proc0000" / "end_state.dat", d / "end_state0000.dat")
+    t_in = (d / "run.in").read_text().replace("restart             = .false.", "restart             = .true.")
+    (d / "run.in").write_text(t_in.replace("end_time            = 0.095", "end_time            = 0.195"))
+    run(d)
+    p2, t2, _, _, psi2 = read_end_state(d / "proc0000" / "end_state.dat")
+    s.solver(10)
+    assert p2 == 20
+    np.testing.assert_array_equal(psi2, s.get_state())
+
+
+def test_host_rejects_existing_end_state(gpu, tmp_path):
+    d = tmp_path / "run"
+    shutil.copytree(INPUTS / "ring64", d)
+    (d / "end_state0000.dat").write_bytes(b"\0" * 64)
+    r = subprocess.run([str(HOST), "--dir", str(d)], capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
+    assert "restart=.false. but end_state0000.dat exists" in (d / "ERROR").read_text()

@@ -1,0 +1,62 @@
+"""The C++ host driver (gpe_b200/bin/gpe_host): parsing of the reference's
+input files and its error convention, on CPU (no GPU needed)."""
+from __future__ import annotations
+
+import json
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from gpe_b200.build import HOST
+
+INPUTS = Path(__file__).resolve().parent / "golden" / "inputs"
+
+
+def run_host(d, *args):
+    return subprocess.run([str(HOST), "--dir", str(d), *args], capture_output=True, text=True, timeout=60)
+
+
+@pytest.fixture
+def ring_dir(tmp_path):
+    d = tmp_path / "ring64"
+    shutil.copytree(INPUTS / "ring64", d)
+    return d
+
+
+def test_parse_reference_inputs(ring_dir):
+    r = run_host(ring_dir, "--parse-only")
+    assert r.returncode == 0, r.stderr
+    p = json.loads(r.stdout)
+    assert (p["nx"], p["ny"], p["nz"], p["pr"]) == (64, 64, 64, 8)
+    assert p["scheme"] == 2 and p["eqn"] == 4 and p["bcs"] == 2 and p["order"] == 2
+    assert p["tau"] == 0.01 and p["end_time"] == 0.095 and p["xr"] == 15.75 and p["save_rate"] == 2
+    assert p["nic"] == 1 and p["ic"][0] == 3  # GPE_IC_RING
+    assert p["ring_r0"] == 4.0 and p["ring_plane"] == "xy"
+
+
+def test_ic_products_and_single_precision(ring_dir):
+    (ring_dir / "ic.in").write_text("  init_cond = fermi() * vortex_line(vl1)\n")
+    pin = (ring_dir / "parameters.in").read_text()
+    pin = pin.replace("  !integer, parameter :: pr = selected_real_kind(6,37)\n  integer, parameter :: pr = "
+                      "selected_real_kind(15,307)", "  integer, parameter :: pr = selected_real_kind(6,37)")
+    (ring_dir / "parameters.in").write_text(pin)
+    p = json.loads(run_host(ring_dir, "--parse-only").stdout)
+    assert p["pr"] == 4 and p["nic"] == 2 and p["ic"][:2] == [1, 2] and p["line_dir"] == "z"
+
+
+def test_unknown_scheme_is_an_emergency_stop(ring_dir):
+    t = (ring_dir / "run.in").read_text().replace("'rk4'", "'rk9'")
+    (ring_dir / "run.in").write_text(t)
+    r = run_host(ring_dir, "--parse-only")
+    assert r.returncode != 0
+    assert "Unrecognised time stepping scheme" in (ring_dir / "ERROR").read_text()
+
+
+def test_missing_namelist_is_an_emergency_stop(ring_dir):
+    t = (ring_dir / "run.in").read_text()
+    (ring_dir / "run.in").write_text(t[: t.index("&misc_params")])
+    r = run_host(ring_dir, "--parse-only")
+    assert r.returncode != 0
+    assert "error reading namelist misc_params" in (ring_dir / "ERROR").read_text()
