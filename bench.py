@@ -322,6 +322,32 @@ def batched_leg(args, torch):
             "timing": "host clock, first submit to last result, uploads/downloads included"}
 
 
+def run_serving(args) -> int:
+    """Serving sample: the first `--requests` requests of the synthetic
+    stream (Poisson 20/s; sizes 48^3..256^3; 200-5000 RK4/RKF45 steps;
+    order 2/4; V = 0 or a trap; ring / line / random-phase ICs; FP64 or FP32
+    storage) served with continuous batching from one HBM budget, then the
+    same requests through the plain one-solve-at-a-time FP64 path."""
+    import torch
+
+    from gpe_b200 import serve
+
+    torch.cuda.set_device(0)
+    reqs = serve.make_requests(args.requests)
+    free, total = torch.cuda.mem_get_info()
+    budget = int(free * 0.85)
+    batched = serve.serve(reqs, budget, chunk=50).summary()
+    single = serve.serve_one_at_a_time(reqs).summary()
+    work = sum(r.sites * r.nsteps for r in reqs)
+    line = {"metric": "serving p50/p99 latency and site-updates/s", "requests": len(reqs),
+            "offered_site_steps": work, "arrival_span_s": reqs[-1].arrival_s,
+            "offered_site_steps_per_s": work / reqs[-1].arrival_s, "budget_bytes": budget,
+            "continuous_batching": batched, "one_at_a_time_fp64": single,
+            "throughput_ratio": batched["site_updates_per_s"] / single["site_updates_per_s"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,12 +359,17 @@ def main() -> int:
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32-storage and RKF45 legs")
     ap.add_argument("--ncu-case", action="store_true",
                     help="profiling target: set up the workload and run 2 RK4 steps, nothing else")
+    ap.add_argument("--serving", action="store_true",
+                    help="serving workload: Poisson stream of mixed solves, continuous batching vs one at a time")
+    ap.add_argument("--requests", type=int, default=40, help="--serving: requests in the sample")
     ap.add_argument("--storage", default="c128", choices=["c128", "c64"],
                     help="storage of the --ncu-case / --quick workload")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    if args.serving:
+        return run_serving(args)
 
     import torch
 

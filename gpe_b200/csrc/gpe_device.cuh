@@ -369,19 +369,37 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
 
     if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 || KIND == K_RK4_2 ||
                   KIND == K_RK4_4) {
-      // out = base + cf0 * f
-      cx<double> base;
-      if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
-      else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
-      else base = cx<double>{cr, ci};
-      const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
-      const S ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
+      // out = base + cf0 * f.  Outputs that are a new psi (Euler, RK2 stage
+      // 2, RK4 stage 4) are formed in FP64; intermediate stage inputs in the
+      // stencil's compute type C (identical to FP64 when C = double).
+      constexpr bool FINAL = (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4);
+      S ns;
+      if constexpr (FINAL || sizeof(C) == sizeof(double)) {
+        cx<double> base;
+        if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
+        else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
+        else base = cx<double>{cr, ci};
+        const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
+        ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
+      } else {
+        const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2) ? to_c<C>(pv) : n.c0;
+        const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
+        ns = to_s<S>(cx<C>{base.r + (ar * f.r - ai * f.i), base.i + (ar * f.i + ai * f.r)});
+      }
       store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
       if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
-        // acc = (psi | acc) + cf1 * f
-        const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
-        const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
-        ((S*)a.acc)[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
+        // acc = (psi | acc) + cf1 * f, in the storage's precision class: the
+        // stored accumulator is rounded to S either way; the last update,
+        // psi_new = acc + dt/6 k4, is the FP64 one above
+        if constexpr (sizeof(C) == sizeof(double)) {
+          const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
+          const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
+          ((S*)a.acc)[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
+        } else {
+          const cx<C> ab = (KIND == K_RK4_1) ? n.c0 : to_c<C>(av);
+          const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
+          ((S*)a.acc)[o] = to_s<S>(cx<C>{ab.r + (br * f.r - bi * f.i), ab.i + (br * f.i + bi * f.r)});
+        }
       }
       if constexpr (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4) {
         if (a.want_norm) {
@@ -389,6 +407,24 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
           r_norm += (cc.wxy * a.wz[k]) * (sr * sr + si * si);
         }
       }
+    } else if constexpr (KIND != K_CK_6 && sizeof(C) != sizeof(double)) {
+      // Cash-Karp stages 1-5 in the stencil's compute type: K_m = dt f and
+      // tmp = psi + sum_j b_j K_j feed the next stencil only
+      const cx<C> Km{(C)a.cf_r[0] * f.r - (C)a.cf_i[0] * f.i, (C)a.cf_r[0] * f.i + (C)a.cf_i[0] * f.r};
+      const S Ks = to_s<S>(Km);
+      ((S*)a.kout)[o] = Ks;
+      const cx<C> Kmc = to_c<C>(Ks);
+      const cx<C> pc = (KIND == K_CK_1) ? n.c0 : to_c<C>(pv);
+      C tr = pc.r, ti = pc.i;
+#pragma unroll
+      for (int m = 0; m < T::NK; ++m) {
+        const cx<C> km = to_c<C>(kv[m]);
+        tr = tr + (C)a.b[m] * km.r;
+        ti = ti + (C)a.b[m] * km.i;
+      }
+      tr = tr + (C)a.b[T::NK] * Kmc.r;
+      ti = ti + (C)a.b[T::NK] * Kmc.i;
+      store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<C>{tr, ti}));
     } else {
       // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
       const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);

@@ -50,6 +50,19 @@ def initial_state(req: Request) -> np.ndarray:
     return psi.astype(np.complex64) if p.storage == "c64" else psi
 
 
+def device_ic(req: Request):
+    """The request's initial state as a device-side IC spec (no host array,
+    no host-to-device copy)."""
+    p = req.params
+    if req.ic_kind == "ring":
+        return ic.device_spec("ring", ring=dict(plane="xy", r0=req.ic_arg))
+    if req.ic_kind == "line":
+        if p.omx or p.omy or p.omz:
+            return ic.device_spec("fermi", "line_pade")
+        return ic.device_spec("line_pade")
+    return ic.device_spec("random_phase", seed=req.seed, kc=req.ic_arg)
+
+
 def make_requests(n: int, rate_per_s: float = 20.0, seed: int = 2024,
                   sizes=tuple(range(48, 257, 16)), steps=(200, 5000)) -> list[Request]:
     """Synthetic request stream: Poisson arrivals; cubic sizes uniform in
@@ -101,11 +114,15 @@ class ServeReport:
 
 
 def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime: bool = True,
-          prep_threads: int = 4) -> ServeReport:
+          prep_threads: int = 4, device_ics: bool = True) -> ServeReport:
     """Run the request stream through one Pool.  With realtime=True a request
     becomes visible at its arrival time on the host clock; every loop turn
     admits what has arrived and fits, advances the batch by up to `chunk`
-    steps, and collects finished solves."""
+    steps, and collects finished solves.  device_ics=True builds each
+    initial state on the GPU at admission; False prepares it on host
+    threads and copies it in."""
+    if device_ics:
+        return _serve_device_ics(requests, budget_bytes, chunk, realtime)
     pool = Pool(budget_bytes)
     rep = ServeReport()
     pending = sorted(requests, key=lambda r: r.arrival_s)
@@ -146,4 +163,65 @@ def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime:
     rep.wall_s = time.perf_counter() - t0
     prep.shutdown()
     pool.close()
+    return rep
+
+
+def _serve_device_ics(requests, budget_bytes, chunk, realtime) -> ServeReport:
+    pool = Pool(budget_bytes)
+    rep = ServeReport()
+    pending = sorted(requests, key=lambda r: r.arrival_s)
+    by_tag = {r.tag: r for r in requests}
+    waiting: list[Request] = []
+    t0 = time.perf_counter()
+    active = 0
+    nxt = 0
+    while nxt < len(pending) or waiting or active:
+        now = time.perf_counter() - t0
+        while nxt < len(pending) and (not realtime or pending[nxt].arrival_s <= now):
+            waiting.append(pending[nxt])
+            nxt += 1
+        still = []
+        for req in waiting:
+            if pool.submit_ic(req.params, device_ic(req), req.nsteps, req.tag):
+                active += 1
+            else:
+                rep.rejected_admissions += 1
+                still.append(req)
+        waiting = still
+        if active == 0:
+            time.sleep(0.002)
+            continue
+        rep.max_active = max(rep.max_active, active)
+        active = pool.step(chunk)
+        done_t = time.perf_counter() - t0
+        for r in pool.poll():
+            req = by_tag[r.tag]
+            rep.latencies_s[r.tag] = done_t - req.arrival_s
+            rep.site_updates += req.sites * r.steps
+    rep.wall_s = time.perf_counter() - t0
+    pool.close()
+    return rep
+
+
+def serve_one_at_a_time(requests: list[Request], realtime: bool = True) -> ServeReport:
+    """Baseline: the plain one-solve-at-a-time FP64 path -- each request runs
+    alone through the single-solve handle (complex128 storage), in arrival
+    order, starting when it has arrived and the previous one has finished."""
+    from .solver import Solver
+
+    rep = ServeReport()
+    t0 = time.perf_counter()
+    for req in sorted(requests, key=lambda r: r.arrival_s):
+        if realtime:
+            wait = req.arrival_s - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+        s = Solver(req.params.replace(storage="c128", compute="auto"))
+        s.set_ic(device_ic(req))
+        s.solver(req.nsteps)
+        s.close()
+        rep.latencies_s[req.tag] = time.perf_counter() - t0 - req.arrival_s
+        rep.site_updates += req.sites * req.nsteps
+        rep.max_active = 1
+    rep.wall_s = time.perf_counter() - t0
     return rep
