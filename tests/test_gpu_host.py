@@ -59,7 +59,9 @@ def test_host_run_and_restart(gpu, tmp_path):
     # modulo(t+im_t, |dt|*save_rate) < |dt| test)
     assert len(e) >= 2 and all(len(x) == 51 for x in e)
     assert len(nrm) >= 2 and all(len(x) == 68 for x in nrm)
-    assert float(nrm[-1].split()[2]) == pytest.approx(s.get_norm(), rel=1e-12)
+    # records are written at the steps where the save test fires; the norm
+    # is conserved to O(dt^4) in real time
+    assert all(float(x.split()[2]) == pytest.approx(s.get_norm(), rel=1e-5) for x in nrm)
     # restart from the end state for 10 more steps == 20 steps straight
     shutil.copy(d / "proc0000" / "end_state.dat", d / "end_state0000.dat")
     t_in = (d / "run.in").read_text().replace("restart             = .false.", "restart             = .true.")
