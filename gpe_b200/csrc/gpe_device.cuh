@@ -50,7 +50,7 @@ struct Geom {
   long long px, pz;     // row and plane pitch in elements
 };
 
-struct StageArgs {
+struct alignas(16) StageArgs {
   Geom g;
   int R;                // stencil radius: 1 (order 2) or 2 (order 4)
   int bcs;              // 1 periodic, 2 reflective
@@ -80,6 +80,8 @@ struct StageArgs {
   double* partials;             // [nblocks][RED_SLOTS]
   int* status;                  // device status word: non-zero = a bounded wait expired
 };
+
+static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is copied in 16-byte words");
 
 template <class S>
 struct Stor;

@@ -168,6 +168,7 @@ struct Class {
   int nitems = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  cudaStream_t st = nullptr;  // classes run concurrently, one stream each
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
@@ -359,8 +360,8 @@ int build_items(gpe_pool* P, Class& c, const std::vector<Solve*>& sv) {
   PCU(P, c.res.ensure(sv.size() * RED_SLOTS));
   PCU(P, c.hres.ensure(sv.size() * RED_SLOTS));
   PCU(P, cudaMemcpyAsync(c.items.p, c.hitems.data(), c.hitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice,
-                         P->st));
-  PCU(P, cudaMemcpyAsync(c.first.p, c.hfirst.data(), c.hfirst.size() * sizeof(int), cudaMemcpyHostToDevice, P->st));
+                         c.st));
+  PCU(P, cudaMemcpyAsync(c.first.p, c.hfirst.data(), c.hfirst.size() * sizeof(int), cudaMemcpyHostToDevice, c.st));
   return GPE_OK;
 }
 
@@ -374,13 +375,21 @@ int check_status(gpe_pool* P) {
   return GPE_OK;
 }
 
-// Advance the RK4 class by `chunk` steps (all its solves).
-int run_rk4(gpe_pool* P, int cm, int64_t chunk) {
+int ensure_stream(gpe_pool* P, Class& c) {
+  if (!c.st) PCU(P, cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+  return GPE_OK;
+}
+
+// Enqueue `chunk` RK4 steps of every solve of an RK4 class on the class's
+// stream (the step is a captured graph of four batched launches), then the
+// per-solve norm of the result; returns without waiting.
+int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
   Class& c = P->cls[cm][FAM_RK4];
   const int ns = (int)c.solves.size();
-  if (!ns || chunk <= 0) return GPE_OK;
+  if (int rc = ensure_stream(P, c)) return rc;
   if (c.dirty) {
     c.drop_graph();
+    PCU(P, cudaStreamSynchronize(c.st));
     if (int rc = build_items(P, c, c.solves)) return rc;
     PCU(P, c.tab.ensure((size_t)4 * ns));
     PCU(P, c.htab.ensure((size_t)4 * ns));
@@ -389,19 +398,19 @@ int run_rk4(gpe_pool* P, int cm, int64_t chunk) {
       rk4_tables(P, c.solves[q], t4.data());
       for (int m = 0; m < 4; ++m) c.htab.p[(size_t)m * ns + q] = t4[m];
     }
-    PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)4 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, P->st));
+    PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)4 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
     const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_2, K_RK4_4};
     int grids[4];
     for (int m = 0; m < 4; ++m) grids[m] = grid_for(cm, kinds[m], c.nitems);
     // capture one RK4 step of the whole class
-    PCU(P, cudaStreamSynchronize(P->st));
-    PCU(P, cudaStreamBeginCapture(P->st, cudaStreamCaptureModeThreadLocal));
+    PCU(P, cudaStreamSynchronize(c.st));
+    PCU(P, cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     for (int m = 0; m < 4 && e == cudaSuccess; ++m)
-      e = launch_batch(cm, kinds[m], grids[m], P->st, c.tab.p + (size_t)m * ns, c.items.p, c.nitems,
+      e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)m * ns, c.items.p, c.nitems,
                        m == 3 ? c.part.p : nullptr, nullptr);
     cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(P->st, &g);
+    cudaError_t e2 = cudaStreamEndCapture(c.st, &g);
     if (e != cudaSuccess || e2 != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       return pfail(P, GPE_ERR_CUDA, std::string("capturing the batched RK4 step failed: ") +
@@ -411,13 +420,18 @@ int run_rk4(gpe_pool* P, int cm, int64_t chunk) {
     PCU(P, cudaGraphInstantiate(&c.gexec, c.graph, 0));
     c.dirty = false;
   }
-  for (int64_t q = 0; q < chunk; ++q) PCU(P, cudaGraphLaunch(c.gexec, P->st));
-  k_finalize_ranges<<<ns, 256, 0, P->st>>>(c.part.p, c.first.p, c.res.p);
+  for (int64_t q = 0; q < chunk; ++q) PCU(P, cudaGraphLaunch(c.gexec, c.st));
+  k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
   PCU(P, cudaGetLastError());
-  PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, P->st));
-  PCU(P, cudaStreamSynchronize(P->st));
-  if (int rc = check_status(P)) return rc;
-  for (int q = 0; q < ns; ++q) {
+  PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  return GPE_OK;
+}
+
+// After rk4_enqueue's work completed: advance the solves' clocks.
+int rk4_collect(gpe_pool* P, int cm, int64_t chunk) {
+  Class& c = P->cls[cm][FAM_RK4];
+  PCU(P, cudaStreamSynchronize(c.st));
+  for (size_t q = 0; q < c.solves.size(); ++q) {
     Solve* s = c.solves[q];
     for (int64_t k = 0; k < chunk; ++k) {
       s->t = s->t + s->dr;
@@ -431,79 +445,83 @@ int run_rk4(gpe_pool* P, int cm, int64_t chunk) {
   return GPE_OK;
 }
 
-// RKF45 attempts for the class until every solve has taken its quota.
-int run_rk45(gpe_pool* P, int cm) {
+// One RKF45 attempt of every solve of an RK45 class that still has quota,
+// enqueued on the class's stream.  *launched = number of solves attempted.
+int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
   Class& c = P->cls[cm][FAM_RK45];
-  if (c.solves.empty()) return GPE_OK;
-  for (int round = 0; round < 100000; ++round) {
-    std::vector<Solve*> sv;
-    for (Solve* s : c.solves)
-      if (s->quota > 0 && s->status == GPE_OK) sv.push_back(s);
-    if (sv.empty()) return GPE_OK;
-    const int ns = (int)sv.size();
-    if (int rc = build_items(P, c, sv)) return rc;
-    PCU(P, c.tab.ensure((size_t)6 * ns));
-    PCU(P, c.htab.ensure((size_t)6 * ns));
-    std::vector<BatchStage> t6(6);
-    for (int q = 0; q < ns; ++q) {
-      rk45_tables(P, sv[q], t6.data());
-      for (int m = 0; m < 6; ++m) c.htab.p[(size_t)m * ns + q] = t6[m];
-    }
-    PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, P->st));
-    for (int m = 0; m < 6; ++m)
-      PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), P->st, c.tab.p + (size_t)m * ns,
-                          c.items.p, c.nitems, m == 5 ? c.part.p : nullptr, nullptr));
-    k_finalize_ranges<<<ns, 256, 0, P->st>>>(c.part.p, c.first.p, c.res.p);
-    PCU(P, cudaGetLastError());
-    PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost,
-                           P->st));
-    PCU(P, cudaStreamSynchronize(P->st));
-    if (int rc = check_status(P)) return rc;
-    for (int q = 0; q < ns; ++q) {
-      Solve* s = sv[q];
-      const gpe_params& p = s->p;
-      const double eps = p.eps != 0 ? p.eps : 1e-6, safety = p.safety != 0 ? p.safety : 0.9;
-      const double dtdec = p.dt_decrease != 0 ? p.dt_decrease : -0.25;
-      const double dtinc = p.dt_increase != 0 ? p.dt_increase : -0.2;
-      const double errcon = pow(5.0 / safety, 1.0 / dtinc);
-      const double errmax = c.hres.p[q * RED_SLOTS + 2] / eps;
-      if (!std::isfinite(errmax)) {
-        s->status = GPE_ERR_NONFINITE;
-        continue;
-      }
-      if (errmax > 1.0) {  // reject: shrink and retry from the same psi
-        s->rejected++;
-        const double e = pow(errmax, dtdec);
-        const double tr = (safety * s->dr) * e, ti = (safety * s->di) * e;
-        const double mm = std::max(hypot(tr, ti), 0.1 * hypot(s->dr, s->di));
-        if (!(s->di == 0.0)) { s->dr = 0.0; s->di = -mm; }  // imaginary time: dt on the negative imaginary axis
-        else { s->dr = mm; s->di = 0.0; }
-        continue;
-      }
-      double nr, ni;
-      if (errmax > errcon) {
-        const double e = pow(errmax, dtinc);
-        nr = (safety * s->dr) * e;
-        ni = (safety * s->di) * e;
-      } else {
-        nr = 5.0 * s->dr;
-        ni = 5.0 * s->di;
-      }
-      s->t = s->t + s->dr;
-      s->dr = nr;
-      s->di = ni;
-      s->im_t = s->im_t + fabs(ni);  // the new dt, as src/solve.f90:229
-      s->errmax = errmax;
-      s->cur = 1 - s->cur;
-      s->p_index += 1;
-      s->done += 1;
-      s->quota -= 1;
-      s->dte_r = s->dr;  // next step's psi_scal uses the dt at rkqs entry
-      s->dte_i = s->di;
-      s->norm = ((c.hres.p[q * RED_SLOTS + 0] * s->d[0]) * s->d[1]) * s->d[2];
-    }
+  sv.clear();
+  for (Solve* s : c.solves)
+    if (s->quota > 0 && s->status == GPE_OK) sv.push_back(s);
+  if (sv.empty()) return GPE_OK;
+  if (int rc = ensure_stream(P, c)) return rc;
+  const int ns = (int)sv.size();
+  if (int rc = build_items(P, c, sv)) return rc;
+  PCU(P, c.tab.ensure((size_t)6 * ns));
+  PCU(P, c.htab.ensure((size_t)6 * ns));
+  std::vector<BatchStage> t6(6);
+  for (int q = 0; q < ns; ++q) {
+    rk45_tables(P, sv[q], t6.data());
+    for (int m = 0; m < 6; ++m) c.htab.p[(size_t)m * ns + q] = t6[m];
   }
-  return pfail(P, GPE_ERR_STATE, "rkqs: no acceptable step after 100000 batched attempts");
+  PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
+  for (int m = 0; m < 6; ++m)
+    PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), c.st, c.tab.p + (size_t)m * ns,
+                        c.items.p, c.nitems, m == 5 ? c.part.p : nullptr, nullptr));
+  k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
+  PCU(P, cudaGetLastError());
+  PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  return GPE_OK;
+}
+
+// rkqs step control (src/solve.f90:184-229) of each attempted solve.
+int rk45_collect(gpe_pool* P, int cm, const std::vector<Solve*>& sv) {
+  Class& c = P->cls[cm][FAM_RK45];
+  PCU(P, cudaStreamSynchronize(c.st));
+  for (size_t q = 0; q < sv.size(); ++q) {
+    Solve* s = sv[q];
+    const gpe_params& p = s->p;
+    const double eps = p.eps != 0 ? p.eps : 1e-6, safety = p.safety != 0 ? p.safety : 0.9;
+    const double dtdec = p.dt_decrease != 0 ? p.dt_decrease : -0.25;
+    const double dtinc = p.dt_increase != 0 ? p.dt_increase : -0.2;
+    const double errcon = pow(5.0 / safety, 1.0 / dtinc);
+    const double errmax = c.hres.p[q * RED_SLOTS + 2] / eps;
+    if (!std::isfinite(errmax)) {
+      s->status = GPE_ERR_NONFINITE;
+      continue;
+    }
+    if (errmax > 1.0) {  // reject: shrink and retry from the same psi
+      s->rejected++;
+      if (s->rejected > 100000) s->status = GPE_ERR_STATE;
+      const double e = pow(errmax, dtdec);
+      const double tr = (safety * s->dr) * e, ti = (safety * s->di) * e;
+      const double mm = std::max(hypot(tr, ti), 0.1 * hypot(s->dr, s->di));
+      if (!(s->di == 0.0)) { s->dr = 0.0; s->di = -mm; }  // imaginary time: dt on the negative imaginary axis
+      else { s->dr = mm; s->di = 0.0; }
+      continue;
+    }
+    double nr, ni;
+    if (errmax > errcon) {
+      const double e = pow(errmax, dtinc);
+      nr = (safety * s->dr) * e;
+      ni = (safety * s->di) * e;
+    } else {
+      nr = 5.0 * s->dr;
+      ni = 5.0 * s->di;
+    }
+    s->t = s->t + s->dr;
+    s->dr = nr;
+    s->di = ni;
+    s->im_t = s->im_t + fabs(ni);  // the new dt, as src/solve.f90:229
+    s->errmax = errmax;
+    s->cur = 1 - s->cur;
+    s->p_index += 1;
+    s->done += 1;
+    s->quota -= 1;
+    s->dte_r = s->dr;  // next step's psi_scal uses the dt at rkqs entry
+    s->dte_i = s->di;
+    s->norm = ((c.hres.p[q * RED_SLOTS + 0] * s->d[0]) * s->d[1]) * s->d[2];
+  }
+  return GPE_OK;
 }
 
 void release_solve(gpe_pool* P, Solve* s) {
@@ -647,20 +665,40 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
     c.dirty = true;
   }
   P->pending.clear();
+  // RK4 classes: enqueue their chunk on their own streams and let them run
+  // while the RKF45 classes go through their attempts
+  int64_t chunks[NCM] = {0};
   for (int cm = 0; cm < NCM; ++cm) {
     Class& c = P->cls[cm][FAM_RK4];
     int64_t chunk = max_steps;
     for (Solve* s : c.solves) chunk = std::min(chunk, s->nsteps - s->done);
-    if (!c.solves.empty() && chunk > 0)
-      if (int rc = run_rk4(P, cm, chunk)) return rc;
-    Class& k = P->cls[cm][FAM_RK45];
-    for (Solve* s : k.solves) {
+    if (!c.solves.empty() && chunk > 0) {
+      if (int rc = rk4_enqueue(P, cm, chunk)) return rc;
+      chunks[cm] = chunk;
+    }
+  }
+  for (int cm = 0; cm < NCM; ++cm)
+    for (Solve* s : P->cls[cm][FAM_RK45].solves) {
       s->quota = std::min(max_steps, s->nsteps - s->done);
       s->dte_r = s->dr;
       s->dte_i = s->di;
     }
-    if (int rc = run_rk45(P, cm)) return rc;
+  for (int round = 0; round < 1000000; ++round) {
+    std::vector<Solve*> sv[NCM];
+    bool any = false;
+    for (int cm = 0; cm < NCM; ++cm) {
+      if (int rc = rk45_enqueue(P, cm, sv[cm])) return rc;
+      any |= !sv[cm].empty();
+    }
+    if (!any) break;
+    for (int cm = 0; cm < NCM; ++cm)
+      if (!sv[cm].empty())
+        if (int rc = rk45_collect(P, cm, sv[cm])) return rc;
   }
+  for (int cm = 0; cm < NCM; ++cm)
+    if (chunks[cm])
+      if (int rc = rk4_collect(P, cm, chunks[cm])) return rc;
+  if (int rc = check_status(P)) return rc;
   // retire finished solves
   int active = 0;
   for (int cm = 0; cm < NCM; ++cm)
@@ -728,6 +766,10 @@ void gpe_pool_destroy(gpe_pool* P) {
       Class& c = P->cls[cm][fam];
       for (Solve* s : c.solves) delete s;
       c.drop_graph();
+      if (c.st) {
+        cudaStreamSynchronize(c.st);
+        cudaStreamDestroy(c.st);
+      }
       c.tab.free();
       c.items.free();
       c.first.free();

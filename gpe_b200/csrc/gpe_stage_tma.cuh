@@ -77,6 +77,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// Copy stage arguments from the device table through the read-only path.
+__device__ __forceinline__ StageArgs __ldg_args(const StageArgs* p) {
+  StageArgs a;
+  const uint4* src = reinterpret_cast<const uint4*>(p);
+  uint4* dst = reinterpret_cast<uint4*>(&a);
+#pragma unroll
+  for (int q = 0; q < (int)(sizeof(StageArgs) / sizeof(uint4)); ++q) dst[q] = __ldg(src + q);
+  return a;
+}
+
 // Order a tensor map that sits in global memory (written by the host
 // between launches) before the async proxy reads it.
 __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
@@ -369,19 +379,19 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_batch(const BatchStage* 
   using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
-  __shared__ StageArgs sa;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   const int tid = threadIdx.y * 32 + threadIdx.x;
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const BatchItem it = items[w];
     const BatchStage* bs = tab + it.solve;
-    __syncthreads();  // previous item is done with sa
     if (tid == 0) {
-      sa = bs->args;
       tensormap_acquire(&bs->maps.in);
       for (int f = 0; f < StageTraits<KIND>::NPW; ++f) tensormap_acquire(&bs->maps.pw[f]);
     }
-    __syncthreads();
+    // the item's arguments in registers (read-only path, same address for
+    // every thread); a shared-memory copy would be re-read after every
+    // barrier of the z march
+    const StageArgs sa = __ldg_args(&bs->args);
     const int R = sa.R;
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;

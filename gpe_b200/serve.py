@@ -114,7 +114,7 @@ class ServeReport:
 
 
 def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime: bool = True,
-          prep_threads: int = 4, device_ics: bool = True) -> ServeReport:
+          prep_threads: int = 4, device_ics: bool = True, max_active_sites: int = 160 << 20) -> ServeReport:
     """Run the request stream through one Pool.  With realtime=True a request
     becomes visible at its arrival time on the host clock; every loop turn
     admits what has arrived and fits, advances the batch by up to `chunk`
@@ -122,7 +122,7 @@ def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime:
     initial state on the GPU at admission; False prepares it on host
     threads and copies it in."""
     if device_ics:
-        return _serve_device_ics(requests, budget_bytes, chunk, realtime)
+        return _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
     pool = Pool(budget_bytes)
     rep = ServeReport()
     pending = sorted(requests, key=lambda r: r.arrival_s)
@@ -166,7 +166,11 @@ def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime:
     return rep
 
 
-def _serve_device_ics(requests, budget_bytes, chunk, realtime) -> ServeReport:
+def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites) -> ServeReport:
+    """Admission is first-come first-served, bounded by the HBM budget and by
+    max_active_sites: enough grid sites in flight to keep the GPU's memory
+    system busy, no more, so that early requests are not slowed by every
+    later arrival."""
     pool = Pool(budget_bytes)
     rep = ServeReport()
     pending = sorted(requests, key=lambda r: r.arrival_s)
@@ -174,6 +178,7 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime) -> ServeReport:
     waiting: list[Request] = []
     t0 = time.perf_counter()
     active = 0
+    active_sites = 0
     nxt = 0
     while nxt < len(pending) or waiting or active:
         now = time.perf_counter() - t0
@@ -181,12 +186,17 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime) -> ServeReport:
             waiting.append(pending[nxt])
             nxt += 1
         still = []
-        for req in waiting:
+        for q, req in enumerate(waiting):
+            if active and active_sites + req.sites > max_active_sites:
+                still.extend(waiting[q:])  # first come, first served
+                break
             if pool.submit_ic(req.params, device_ic(req), req.nsteps, req.tag):
                 active += 1
+                active_sites += req.sites
             else:
                 rep.rejected_admissions += 1
-                still.append(req)
+                still.extend(waiting[q:])
+                break
         waiting = still
         if active == 0:
             time.sleep(0.002)
@@ -198,6 +208,7 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime) -> ServeReport:
             req = by_tag[r.tag]
             rep.latencies_s[r.tag] = done_t - req.arrival_s
             rep.site_updates += req.sites * r.steps
+            active_sites -= req.sites
     rep.wall_s = time.perf_counter() - t0
     pool.close()
     return rep
