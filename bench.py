@@ -227,10 +227,13 @@ def fp32_storage_leg(args, torch, psi0):
         prof = read_profile(s)
         s.close()
         n_sites = rp.nx * rp.ny * rp.nz
-        tot, cnt, bps = prof["rk4_23"]
+        step_bytes = sum(v[2] * v[1] for v in prof.values()) * n_sites
+        step_ms = sum(v[0] for v in prof.values())
         out[compute + "_compute"] = {
-            "value": n_sites * CHUNK * n / (ms * 1e-3), "unit": UNIT, "bytes_per_site_step": 128,
-            "stage23_gbs": bps * n_sites / (tot / cnt * 1e-3) / 1e9,
+            "value": n_sites * CHUNK * n / (ms * 1e-3), "unit": UNIT,
+            "bytes_per_site_step": sum(v[2] * v[1] for v in prof.values()) / (CHUNK * n),
+            "all_stage_kernels_gbs": step_bytes / (step_ms * 1e-3) / 1e9,
+            "per_kind_gbs": {k: v[2] * n_sites / (v[0] / v[1] * 1e-3) / 1e9 for k, v in prof.items()},
             "per_kind_ms": {k: v[0] / v[1] for k, v in prof.items()}}
     return out
 
@@ -423,17 +426,20 @@ def main() -> int:
     prof = read_profile(s)
     s.lib.gpe_profile(s.h, 0)
 
-    # roofline of the dominant kernel: the RK4 stage-2/3 kernel (80 B/site)
-    tot, n, bps = prof["rk4_23"]
+    # roofline of the dominant kernel: the stage kind with the largest share
+    # of the step's device time
+    dom = max(prof, key=lambda k: prof[k][0])
+    tot, n, bps = prof[dom]
     avg_ms = tot / n
     achieved = bps * n_sites / (avg_ms * 1e-3) / 1e9
     peak, peak_src = measured_hbm_peak()
-    traffic_ps = ncu_traffic_per_site("rk4_23")
+    traffic_ps = ncu_traffic_per_site(dom)
     step_bytes = sum(v[2] * v[1] for v in prof.values()) * n_sites
     step_ms = sum(v[0] for v in prof.values())
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": (traffic_ps * n_sites) if traffic_ps else None,
-                "kernel": "k_stage<double2,double,R=2,RK4_2,TY=8> (RK4 stages 2 and 3)",
+                "kernel": f"k_stage_tma<double2,double,R=2,{dom.upper()}> (RK4 stage {dom[-1]})",
+                "share": tot / sum(v[0] for v in prof.values()),
                 "bytes_per_site": bps, "avg_launch_ms": avg_ms, "peak_source": peak_src,
                 "frac_of_vendor_8000": achieved / 8000.0,
                 "all_stage_kernels_gbs": step_bytes / (step_ms * 1e-3) / 1e9,

@@ -119,8 +119,8 @@ _PROTOS = {
                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
 }
 
-KIND_NAMES = ["euler", "rk2_1", "rk2_2", "rk4_1", "rk4_23", "rk4_4", "ck_1", "ck_2", "ck_3", "ck_4", "ck_5",
-              "ck_6", "energy"]
+KIND_NAMES = ["euler", "rk2_1", "rk2_2", "rk4_1", "rk4_2", "rk4_4", "ck_1", "ck_2", "ck_3", "ck_4", "ck_5",
+              "ck_6", "energy", "rk4_3"]
 
 _lib = None
 

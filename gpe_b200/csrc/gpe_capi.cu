@@ -131,8 +131,8 @@ cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a_in) {
   if (fin < 0) return cudaErrorInvalidValue;
   m.in = h->map_halo[fin];
   // point-wise inputs in the order of StageTraits: psi, acc, K...
-  const bool has_psi = (kind == K_RK2_2 || kind == K_RK4_2 || (kind >= K_CK_2 && kind <= K_CK_6));
-  const bool has_acc = (kind == K_RK4_2 || kind == K_RK4_4);
+  const bool has_psi = (kind == K_RK2_2 || kind == K_RK4_2 || kind == K_RK4_3 || (kind >= K_CK_2 && kind <= K_CK_6));
+  const bool has_acc = (kind == K_RK4_4);
   const int nk = (kind >= K_CK_2 && kind <= K_CK_5) ? (kind - K_CK_1) : (kind == K_CK_6 ? 4 : 0);
   int q = 0;
   const void* pws[7];
@@ -237,27 +237,26 @@ int enqueue_fixed_step(gpe_handle* h, double dr, double di, bool energy, bool no
   void** F = h->fields.data();
   const int sc = h->p.scheme;
   if (sc == GPE_RK4) {
-    void *psi = F[0], *A = F[1], *B = F[2], *acc = F[3];
-    // s1: k1 = f(psi); A = psi + dt/2 k1; acc = psi + dt/6 k1
-    a.in = psi; a.out = A; a.acc = acc;
+    void *psi = F[0], *A = F[1], *B = F[2], *Q = F[3];
+    // s1: k1 = f(psi); A = psi + dt/2 k1
+    a.in = psi; a.out = A;
     a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
-    a.cf_r[1] = dr / 6.0; a.cf_i[1] = di / 6.0;
     a.want_energy = energy;
     a.partials = energy ? h->part_a : nullptr;
     CU(h, launch(h, K_RK4_1, a));
     if (energy && finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
     a.want_energy = 0;
     a.partials = nullptr;
-    // s2: k2 = f(A); B = psi + dt/2 k2; acc += dt/3 k2
-    a.in = A; a.psi = psi; a.out = B;
+    // s2: k2 = f(A); B = psi + dt/2 k2; Q = (psi + A)/3 + dt/3 k2
+    a.in = A; a.psi = psi; a.out = B; a.acc = Q;
     a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
     a.cf_r[1] = dr / 3.0; a.cf_i[1] = di / 3.0;
     CU(h, launch(h, K_RK4_2, a));
-    // s3: k3 = f(B); A = psi + dt k3; acc += dt/3 k3
+    // s3: k3 = f(B); A = psi + dt k3
     a.in = B; a.out = A;
     a.cf_r[0] = dr; a.cf_i[0] = di;
-    CU(h, launch(h, K_RK4_2, a));
-    // s4: k4 = f(A); psi = acc + dt/6 k4
+    CU(h, launch(h, K_RK4_3, a));
+    // s4: k4 = f(A); psi = Q + A/3 + dt/6 k4 (psi itself is not read)
     a.in = A; a.psi = nullptr; a.out = psi;
     a.cf_r[0] = dr / 6.0; a.cf_i[0] = di / 6.0;
     a.want_norm = norm;

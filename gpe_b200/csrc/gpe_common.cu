@@ -113,8 +113,9 @@ int kind_elems(int kind) {
     case K_EULER: return 2;
     case K_RK2_1: return 2;
     case K_RK2_2: return 3;
-    case K_RK4_1: return 3;
-    case K_RK4_2: return 5;
+    case K_RK4_1: return 2;
+    case K_RK4_2: return 4;
+    case K_RK4_3: return 3;
     case K_RK4_4: return 3;
     case K_CK_1: return 3;
     case K_CK_2: return 5;

@@ -29,7 +29,7 @@ enum StageKind : int {
   K_RK2_1,
   K_RK2_2,
   K_RK4_1,
-  K_RK4_2,  // also used for RK4 stage 3 (same data flow, other coefficient)
+  K_RK4_2,
   K_RK4_4,
   K_CK_1,
   K_CK_2,
@@ -38,6 +38,7 @@ enum StageKind : int {
   K_CK_5,
   K_CK_6,
   K_ENERGY,  // no stores: energy of the input state only
+  K_RK4_3,
   K_NUM
 };
 
@@ -296,8 +297,9 @@ __device__ __forceinline__ void block_reduce_store_at(double v0, double v1, doub
 // ---------------------------------------------------------------------------
 template <int KIND>
 struct StageTraits {
-  static constexpr bool HAS_PSI = (KIND == K_RK2_2 || KIND == K_RK4_2 || (KIND >= K_CK_2 && KIND <= K_CK_6));
-  static constexpr bool HAS_ACC = (KIND == K_RK4_2 || KIND == K_RK4_4);
+  static constexpr bool HAS_PSI = (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3 ||
+                                   (KIND >= K_CK_2 && KIND <= K_CK_6));
+  static constexpr bool HAS_ACC = (KIND == K_RK4_4);
   // Cash-Karp K inputs: stages 2..5 read K_1..K_{m-1}; stage 6 reads K1, K3,
   // K4, K5 (K2 only enters with the zero weights c2 = dc2 = 0).
   static constexpr int NK = (KIND >= K_CK_2 && KIND <= K_CK_5) ? (KIND - K_CK_1) : (KIND == K_CK_6 ? 4 : 0);
@@ -370,40 +372,59 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
     S* out = (S*)a.out;
 
     if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 || KIND == K_RK4_2 ||
-                  KIND == K_RK4_4) {
-      // out = base + cf0 * f.  Outputs that are a new psi (Euler, RK2 stage
-      // 2, RK4 stage 4) are formed in FP64; intermediate stage inputs in the
-      // stencil's compute type C (identical to FP64 when C = double).
+                  KIND == K_RK4_3 || KIND == K_RK4_4) {
+      // out = base + cf0 * f, with base = psi_n (pv), the stencil centre, or
+      // for RK4 stage 4 the accumulator plus a third of the centre.  Outputs
+      // that are a new psi (Euler, RK2 stage 2, RK4 stage 4) are formed in
+      // FP64; intermediate stage inputs in the stencil's compute type C
+      // (identical to FP64 when C = double).
+      //
+      // RK4 runs in a reduced-traffic form of classical RK4 (h = dt):
+      //   s1: A = psi + h/2 k1
+      //   s2: B = psi + h/2 k2,  Q = (psi + A)/3 + h/3 k2  (= 2psi/3 + h/6 k1 + h/3 k2)
+      //   s3: A = psi + h k3
+      //   s4: psi' = Q + A/3 + h/6 k4  (= psi + h (k1/6 + k2/3 + k3/3 + k4/6))
+      // so that stage 1 reads 1 field, stage 3 reads 2 and stage 4 reads 2
+      // (solve.f90:124-148 keeps k1..k4; the sum is the same).
       constexpr bool FINAL = (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4);
+      constexpr double THIRD = 1.0 / 3.0;
       S ns;
       if constexpr (FINAL || sizeof(C) == sizeof(double)) {
         cx<double> base;
-        if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2) base = to_c<double>(pv);
-        else if constexpr (KIND == K_RK4_4) base = to_c<double>(av);
-        else base = cx<double>{cr, ci};
+        if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) {
+          base = to_c<double>(pv);
+        } else if constexpr (KIND == K_RK4_4) {
+          const cx<double> qv = to_c<double>(av);
+          base = cx<double>{qv.r + THIRD * cr, qv.i + THIRD * ci};
+        } else {
+          base = cx<double>{cr, ci};
+        }
         const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
         ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
       } else {
-        const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2) ? to_c<C>(pv) : n.c0;
+        const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) ? to_c<C>(pv) : n.c0;
         const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
         ns = to_s<S>(cx<C>{base.r + (ar * f.r - ai * f.i), base.i + (ar * f.i + ai * f.r)});
       }
       store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
-      if constexpr (KIND == K_RK4_1 || KIND == K_RK4_2) {
-        // acc = (psi | acc) + cf1 * f, in the storage's precision class: the
-        // stored accumulator is rounded to S either way; the last update,
-        // psi_new = acc + dt/6 k4, is the FP64 one above
+      if constexpr (KIND == K_RK4_2) {
+        // Q = (psi + A)/3 + h/3 k2 in the storage's precision class: Q is
+        // rounded to S either way; the last update is the FP64 one above
         if constexpr (sizeof(C) == sizeof(double)) {
-          const cx<double> ab = (KIND == K_RK4_1) ? cx<double>{cr, ci} : to_c<double>(av);
+          const cx<double> pd = to_c<double>(pv);
           const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
-          ((S*)a.acc)[o] = to_s<S>(cx<double>{ab.r + t1.r, ab.i + t1.i});
+          ((S*)a.acc)[o] = to_s<S>(cx<double>{(pd.r + cr) * THIRD + t1.r, (pd.i + ci) * THIRD + t1.i});
         } else {
-          const cx<C> ab = (KIND == K_RK4_1) ? n.c0 : to_c<C>(av);
+          // the third is taken in FP64: a C-rounded 1/3 would scale psi by a
+          // biased factor every step (a norm drift of ~1e-7 per step in FP32)
+          const cx<C> pc = to_c<C>(pv);
           const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
-          ((S*)a.acc)[o] = to_s<S>(cx<C>{ab.r + (br * f.r - bi * f.i), ab.i + (br * f.i + bi * f.r)});
+          const double qr = ((double)pc.r + cr) * THIRD + (double)(br * f.r - bi * f.i);
+          const double qi = ((double)pc.i + ci) * THIRD + (double)(br * f.i + bi * f.r);
+          ((S*)a.acc)[o] = to_s<S>(cx<double>{qr, qi});
         }
       }
-      if constexpr (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4) {
+      if constexpr (FINAL) {
         if (a.want_norm) {
           const double sr = (double)ns.x, si = (double)ns.y;
           r_norm += (cc.wxy * a.wz[k]) * (sr * sr + si * si);
@@ -551,9 +572,7 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
   S pv[NPW];
 #pragma unroll
   for (int m = 0; m < T::NPW; ++m)
-    pv[m] = active ? (T::HAS_ACC && m == (T::HAS_PSI ? 1 : 0) ? pwp[m][(long long)(kb + 2) * g.pz + col]
-                                                              : ldro(pwp[m] + (long long)(kb + 2) * g.pz + col))
-                   : szero<S>();
+    pv[m] = active ? ldro(pwp[m] + (long long)(kb + 2) * g.pz + col) : szero<S>();
 
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
 
@@ -569,9 +588,7 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
       for (int h = 0; h < HPT; ++h) hn[h] = hok[h] ? ldro(in + (long long)(k + 3) * g.pz + hcol[h]) : szero<S>();
 #pragma unroll
       for (int m = 0; m < T::NPW; ++m)
-        pn[m] = active ? (T::HAS_ACC && m == (T::HAS_PSI ? 1 : 0) ? pwp[m][(long long)(k + 3) * g.pz + col]
-                                                                  : ldro(pwp[m] + (long long)(k + 3) * g.pz + col))
-                       : szero<S>();
+        pn[m] = active ? ldro(pwp[m] + (long long)(k + 3) * g.pz + col) : szero<S>();
     }
 
     __syncthreads();

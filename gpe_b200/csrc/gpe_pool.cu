@@ -282,25 +282,23 @@ BatchStage make_stage(gpe_pool* P, Solve* s, int kind, int fin, int fout, std::i
   return b;
 }
 
-// RK4 tables: 4 stages (fields psi=0, A=1, B=2, acc=3)
+// RK4 tables: 4 stages (fields psi=0, A=1, B=2, Q=3) of the reduced-traffic
+// RK4 form of site_stage: A = psi + h/2 k1; B = psi + h/2 k2,
+// Q = (psi + A)/3 + h/3 k2; A = psi + h k3; psi = Q + A/3 + h/6 k4
 void rk4_tables(gpe_pool* P, Solve* s, BatchStage* t4) {
   const double dr = s->dr, di = s->di;
   BatchStage b = make_stage(P, s, K_RK4_1, 0, 1, {});
-  b.args.acc = s->f[3];
   b.args.cf_r[0] = 0.5 * dr; b.args.cf_i[0] = 0.5 * di;
-  b.args.cf_r[1] = dr / 6.0; b.args.cf_i[1] = di / 6.0;
   t4[0] = b;
-  b = make_stage(P, s, K_RK4_2, 1, 2, {0, 3});
+  b = make_stage(P, s, K_RK4_2, 1, 2, {0});
   b.args.psi = s->f[0];
   b.args.acc = s->f[3];
   b.args.cf_r[0] = 0.5 * dr; b.args.cf_i[0] = 0.5 * di;
   b.args.cf_r[1] = dr / 3.0; b.args.cf_i[1] = di / 3.0;
   t4[1] = b;
-  b = make_stage(P, s, K_RK4_2, 2, 1, {0, 3});
+  b = make_stage(P, s, K_RK4_3, 2, 1, {0});
   b.args.psi = s->f[0];
-  b.args.acc = s->f[3];
   b.args.cf_r[0] = dr; b.args.cf_i[0] = di;
-  b.args.cf_r[1] = dr / 3.0; b.args.cf_i[1] = di / 3.0;
   t4[2] = b;
   b = make_stage(P, s, K_RK4_4, 1, 0, {3});
   b.args.acc = s->f[3];
@@ -399,7 +397,7 @@ int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
       for (int m = 0; m < 4; ++m) c.htab.p[(size_t)m * ns + q] = t4[m];
     }
     PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)4 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
-    const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_2, K_RK4_4};
+    const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_3, K_RK4_4};
     int grids[4];
     for (int m = 0; m < 4; ++m) grids[m] = grid_for(cm, kinds[m], c.nitems);
     // capture one RK4 step of the whole class

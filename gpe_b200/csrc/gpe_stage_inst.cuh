@@ -24,6 +24,7 @@ static cudaError_t launch_kind(int kind, dim3 grid, cudaStream_t st, const Stage
     GPE_CASE(K_RK2_2)
     GPE_CASE(K_RK4_1)
     GPE_CASE(K_RK4_2)
+    GPE_CASE(K_RK4_3)
     GPE_CASE(K_RK4_4)
     GPE_CASE(K_CK_1)
     GPE_CASE(K_CK_2)
@@ -66,6 +67,7 @@ static cudaError_t launch_tma_kind(int kind, dim3 grid, cudaStream_t st, const T
     GPE_TCASE(K_RK2_2)
     GPE_TCASE(K_RK4_1)
     GPE_TCASE(K_RK4_2)
+    GPE_TCASE(K_RK4_3)
     GPE_TCASE(K_RK4_4)
     GPE_TCASE(K_CK_1)
     GPE_TCASE(K_CK_2)
@@ -142,6 +144,7 @@ static cudaError_t launch_batch_impl(int kind, int grid, cudaStream_t st, const 
     return launch_batch_one<S, C, K>(grid, st, tab, items, nitems, partials);
     GPE_BCASE(K_RK4_1)
     GPE_BCASE(K_RK4_2)
+    GPE_BCASE(K_RK4_3)
     GPE_BCASE(K_RK4_4)
     GPE_BCASE(K_CK_1)
     GPE_BCASE(K_CK_2)

@@ -192,12 +192,13 @@ int gpe_set_ic(gpe_handle* h, const gpe_ic* ic);
 #define GPE_KIND_RK2_1 1
 #define GPE_KIND_RK2_2 2
 #define GPE_KIND_RK4_1 3
-#define GPE_KIND_RK4_23 4
+#define GPE_KIND_RK4_2 4
 #define GPE_KIND_RK4_4 5
 #define GPE_KIND_CK_1 6
 #define GPE_KIND_CK_6 11
 #define GPE_KIND_ENERGY 12
-#define GPE_NUM_KINDS 13
+#define GPE_KIND_RK4_3 13
+#define GPE_NUM_KINDS 14
 
 /* Instrumentation (no reference counterpart; the reference has no tracing
  * beyond timestep.dat, src/solve.f90:234-241): with enable = 1, every stage
