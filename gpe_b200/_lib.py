@@ -10,7 +10,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgpe_cuda.so"
+# GPE_CUDA_LIB selects another build of the library (default: the in-tree one)
+LIB_PATH = Path(os.environ.get("GPE_CUDA_LIB") or Path(__file__).resolve().parent / "lib" / "libgpe_cuda.so")
 
 GPE_OK = 0
 GPE_ERR_BADARG = -1

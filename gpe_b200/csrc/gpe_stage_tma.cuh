@@ -138,7 +138,10 @@ struct TmaRing {
 
 template <class LY>
 __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* s_abort) {
-  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  // align by pointer arithmetic on the __shared__ array itself (an integer
+  // round trip would hide the state space and turn every ring read into a
+  // generic load)
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
   TmaRing rg;
   rg.sbar = (uint64_t*)smem;
   rg.pbar = rg.sbar + LY::NSS;
@@ -237,7 +240,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   }
 
   auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
-  S q[PY][2 * R + 1];
+  S q[PY][2 * R + 1];  // z queue of each owned row: planes k-R .. k+R
   bool ok = true;
 #pragma unroll
   for (int l = 0; l < 2 * R; ++l) {
