@@ -176,54 +176,6 @@ __device__ __forceinline__ cx<C> d1(cx<C> m2, cx<C> m1, cx<C> p1, cx<C> p2, C in
   return o;
 }
 
-// GP right-hand side at one site (solve.f90:414-437)
-// vxy = vx[i] + vy[j] and sxy = sx[i] + sy[j] are hoisted out of the z loop;
-// the sums keep the reference's left-to-right order.
-template <class C>
-__device__ __forceinline__ cx<C> gp_rhs(const StageArgs& a, cx<C> p, cx<C> lap, cx<C> dpx, double vxy,
-                                        double sxy, int i, int j, int k) {
-  cx<C> r;
-  const C n2 = p.r * p.r + p.i * p.i;
-  if (a.eqn == 4) {
-    // -(i + gamma) * (-0.5 lap + V psi + g |psi|^2 psi - mu psi)
-    const C v = (C)(0.5 * (vxy + a.vz[k]));
-    const C g = (C)a.g_nl, mu = (C)a.mu;
-    const C wr = ((-(C)0.5 * lap.r + v * p.r) + g * (n2 * p.r)) - mu * p.r;
-    const C wi = ((-(C)0.5 * lap.i + v * p.i) + g * (n2 * p.i)) - mu * p.i;
-    const C gm = (C)a.gamma;
-    r.r = wi - gm * wr;
-    r.i = -wr - gm * wi;
-  } else if (a.eqn == 2) {
-    // i (lap - |psi|^2 psi) + U dpsi/dx
-    const C cr = lap.r - n2 * p.r, ci = lap.i - n2 * p.i;
-    r.r = -ci;
-    r.i = cr;
-    if (a.has_urhs) {
-      r.r += (C)a.urhs * dpx.r;
-      r.i += (C)a.urhs * dpx.i;
-    }
-  } else {
-    // 0.5 (i + diss) (lap + (1 - |psi|^2) psi) + U dpsi/dx   [eqn 3: * sphere]
-    const C s = (C)1 - n2;
-    const C cr = lap.r + s * p.r, ci = lap.i + s * p.i;
-    C dd = 0;
-    if (a.has_diss) dd = (C)(0.5 * (a.diss_amp * (sxy + a.sz[k])));
-    r.r = dd * cr - (C)0.5 * ci;
-    r.i = dd * ci + (C)0.5 * cr;
-    if (a.has_urhs) {
-      r.r += (C)a.urhs * dpx.r;
-      r.i += (C)a.urhs * dpx.i;
-    }
-    if (a.eqn == 3) {
-      const double xx = a.cx[i], yy = a.cy[j], zz = a.cz[k];
-      const C sp = (C)(0.5 * (1.0 + tanh((sqrt((xx * xx + yy * yy) + zz * zz) - 10.0) - 2.0)));
-      r.r *= sp;
-      r.i *= sp;
-    }
-  }
-  return r;
-}
-
 __device__ __forceinline__ cx<double> cmuld(double ar, double ai, cx<double> b) {
   return cx<double>{ar * b.r - ai * b.i, ar * b.i + ai * b.r};
 }
@@ -316,7 +268,7 @@ struct Nb {
 
 // Per-column constants hoisted out of the z loop.
 struct ColumnConsts {
-  double wxy, vxy, sxy;
+  double wxy, vxy, sxy, rxy2;
   int gx, gy;
 };
 
@@ -325,174 +277,296 @@ __device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i,
   c.wxy = active ? a.wx[i] * a.wy[j] : 0.0;
   c.vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
   c.sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
+  c.rxy2 = (active && a.eqn == 3) ? a.cx[i] * a.cx[i] + a.cy[j] * a.cy[j] : 0.0;
   c.gx = ghost_pos(i, a.g.nx, R, a.bcs);
   c.gy = ghost_pos(j, a.g.ny, R, a.bcs);
   return c;
 }
 
-// Everything a stage does at one interior site (i,j,k) once its stencil
-// neighbourhood and point-wise inputs are in registers: Laplacian, GP
-// right-hand side, the stage combination, the stores (with ghosts) and the
-// fused reductions.  pw[] holds the point-wise inputs in the order
-// psi, acc, K... of StageTraits.
-// o is the element offset of (i,j,k); gz = ghost_pos(k, nz, R, bcs).
-template <class S, class C, int R, int KIND>
-__device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, const S* pw, int i, int j, int k,
-                                           long long o, int gz, const ColumnConsts& cc, double& r_norm,
-                                           double& r_en, double& r_err) {
+// GP right-hand side (solve.f90:414-437) at the PY sites (i, j_r, k) of one
+// thread.  Every statement runs over all PY sites inside the (warp-uniform)
+// equation branches, so the sites' dependency chains interleave.  The
+// column parts of the trap, dissipation and sphere terms come hoisted in cc;
+// the sums keep the reference's left-to-right order.
+template <class C, int PY>
+__device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY], const cx<C> (&lap)[PY],
+                                         const cx<C> (&dpx)[PY], const ColumnConsts (&cc)[PY], int k,
+                                         cx<C> (&r)[PY]) {
+  C n2[PY];
+#pragma unroll
+  for (int q = 0; q < PY; ++q) n2[q] = p[q].r * p[q].r + p[q].i * p[q].i;
+  if (a.eqn == 4) {
+    // -(i + gamma) * (-0.5 lap + V psi + g |psi|^2 psi - mu psi)
+    const double vz = a.vz[k];
+    const C g = (C)a.g_nl, mu = (C)a.mu, gm = (C)a.gamma;
+#pragma unroll
+    for (int q = 0; q < PY; ++q) {
+      const C v = (C)(0.5 * (cc[q].vxy + vz));
+      const C wr = ((-(C)0.5 * lap[q].r + v * p[q].r) + g * (n2[q] * p[q].r)) - mu * p[q].r;
+      const C wi = ((-(C)0.5 * lap[q].i + v * p[q].i) + g * (n2[q] * p[q].i)) - mu * p[q].i;
+      r[q].r = wi - gm * wr;
+      r[q].i = -wr - gm * wi;
+    }
+  } else if (a.eqn == 2) {
+    // i (lap - |psi|^2 psi) + U dpsi/dx
+#pragma unroll
+    for (int q = 0; q < PY; ++q) {
+      const C cr = lap[q].r - n2[q] * p[q].r, ci = lap[q].i - n2[q] * p[q].i;
+      r[q].r = -ci;
+      r[q].i = cr;
+    }
+    if (a.has_urhs) {
+      const C u = (C)a.urhs;
+#pragma unroll
+      for (int q = 0; q < PY; ++q) {
+        r[q].r += u * dpx[q].r;
+        r[q].i += u * dpx[q].i;
+      }
+    }
+  } else {
+    // 0.5 (i + diss) (lap + (1 - |psi|^2) psi) + U dpsi/dx   [eqn 3: * sphere]
+    C dd[PY];
+#pragma unroll
+    for (int q = 0; q < PY; ++q) dd[q] = 0;
+    if (a.has_diss) {
+      const double sz = a.sz[k];
+#pragma unroll
+      for (int q = 0; q < PY; ++q) dd[q] = (C)(0.5 * (a.diss_amp * (cc[q].sxy + sz)));
+    }
+#pragma unroll
+    for (int q = 0; q < PY; ++q) {
+      const C sf = (C)1 - n2[q];
+      const C cr = lap[q].r + sf * p[q].r, ci = lap[q].i + sf * p[q].i;
+      r[q].r = dd[q] * cr - (C)0.5 * ci;
+      r[q].i = dd[q] * ci + (C)0.5 * cr;
+    }
+    if (a.has_urhs) {
+      const C u = (C)a.urhs;
+#pragma unroll
+      for (int q = 0; q < PY; ++q) {
+        r[q].r += u * dpx[q].r;
+        r[q].i += u * dpx[q].i;
+      }
+    }
+    if (a.eqn == 3) {
+      const double zz = a.cz[k];
+#pragma unroll
+      for (int q = 0; q < PY; ++q) {
+        const C sp = (C)(0.5 * (1.0 + tanh((sqrt(cc[q].rxy2 + zz * zz) - 10.0) - 2.0)));
+        r[q].r *= sp;
+        r[q].i *= sp;
+      }
+    }
+  }
+}
+
+// Everything a stage does at the PY interior sites (i, j_q, k) of one thread
+// once their stencil neighbourhoods and point-wise inputs are in registers:
+// Laplacian, GP right-hand side, the stage combination, the stores (with
+// ghosts) and the fused reductions.  pw[q][] holds site q's point-wise
+// inputs in the order psi, acc, K... of StageTraits; o[q] is the element
+// offset of (i, j_q, k); gz = ghost_pos(k, nz, R, bcs).  Sites with
+// act[q] false (outside the grid) are computed but neither stored nor
+// reduced, which keeps the arithmetic free of per-site branches.
+template <class S, class C, int R, int KIND, int PY, int NPWX>
+__device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)[PY], const S (&pw)[PY][NPWX],
+                                            const bool (&act)[PY], int i, const int (&j)[PY], int k,
+                                            const long long (&o)[PY], int gz, const ColumnConsts (&cc)[PY],
+                                            double& r_norm, double& r_en, double& r_err) {
   using T = StageTraits<KIND>;
   const Geom& g = a.g;
-  const cx<C> lxx = d2<C, R>(n.xm2, n.xm1, n.c0, n.xp1, n.xp2, (C)a.ixx);
-  const cx<C> lyy = d2<C, R>(n.ym2, n.ym1, n.c0, n.yp1, n.yp2, (C)a.iyy);
-  const cx<C> lzz = d2<C, R>(n.zm2, n.zm1, n.c0, n.zp1, n.zp2, (C)a.izz);
-  cx<C> lap;
-  lap.r = (lxx.r + lyy.r) + lzz.r;
-  lap.i = (lxx.i + lyy.i) + lzz.i;
-
-  const double cr = (double)n.c0.r, ci = (double)n.c0.i;
+  cx<C> lap[PY], c0[PY];
+#pragma unroll
+  for (int q = 0; q < PY; ++q) {
+    const cx<C> lxx = d2<C, R>(n[q].xm2, n[q].xm1, n[q].c0, n[q].xp1, n[q].xp2, (C)a.ixx);
+    const cx<C> lyy = d2<C, R>(n[q].ym2, n[q].ym1, n[q].c0, n[q].yp1, n[q].yp2, (C)a.iyy);
+    const cx<C> lzz = d2<C, R>(n[q].zm2, n[q].zm1, n[q].c0, n[q].zp1, n[q].zp2, (C)a.izz);
+    lap[q].r = (lxx.r + lyy.r) + lzz.r;
+    lap[q].i = (lxx.i + lyy.i) + lzz.i;
+    c0[q] = n[q].c0;
+  }
 
   if constexpr (T::FIRST) {
     if (a.want_energy) {
       // real(-lap * conjg(psi) + 0.5 |psi|^4)   (variables.f90:591-592)
-      const double n2 = cr * cr + ci * ci;
-      r_en += (-(double)lap.r * cr - (double)lap.i * ci) + 0.5 * (n2 * n2);
+#pragma unroll
+      for (int q = 0; q < PY; ++q) {
+        const double cr = (double)c0[q].r, ci = (double)c0[q].i;
+        const double n2 = cr * cr + ci * ci;
+        const double e = (-(double)lap[q].r * cr - (double)lap[q].i * ci) + 0.5 * (n2 * n2);
+        if (act[q]) r_en += e;
+      }
     }
   }
   if constexpr (KIND != K_ENERGY) {
-    S pv = szero<S>(), av = szero<S>();
-    int q = 0;
-    if constexpr (T::HAS_PSI) pv = pw[q++];
-    if constexpr (T::HAS_ACC) av = pw[q++];
-    const S* kv = pw + q;
-
-    cx<C> dpx{0, 0};
-    if (a.has_urhs) dpx = d1<C, R>(n.xm2, n.xm1, n.xp1, n.xp2, (C)a.ix1);
-    const cx<C> f = gp_rhs<C>(a, n.c0, lap, dpx, cc.vxy, cc.sxy, i, j, k);
-    const cx<double> fd{(double)f.r, (double)f.i};
-    S* out = (S*)a.out;
-
-    if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 || KIND == K_RK4_2 ||
-                  KIND == K_RK4_3 || KIND == K_RK4_4) {
-      // out = base + cf0 * f, with base = psi_n (pv), the stencil centre, or
-      // for RK4 stage 4 the accumulator plus a third of the centre.  Outputs
-      // that are a new psi (Euler, RK2 stage 2, RK4 stage 4) are formed in
-      // FP64; intermediate stage inputs in the stencil's compute type C
-      // (identical to FP64 when C = double).
-      //
-      // RK4 runs in a reduced-traffic form of classical RK4 (h = dt):
-      //   s1: A = psi + h/2 k1
-      //   s2: B = psi + h/2 k2,  Q = (psi + A)/3 + h/3 k2  (= 2psi/3 + h/6 k1 + h/3 k2)
-      //   s3: A = psi + h k3
-      //   s4: psi' = Q + A/3 + h/6 k4  (= psi + h (k1/6 + k2/3 + k3/3 + k4/6))
-      // so that stage 1 reads 1 field, stage 3 reads 2 and stage 4 reads 2
-      // (solve.f90:124-148 keeps k1..k4; the sum is the same).
-      constexpr bool FINAL = (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4);
-      constexpr double THIRD = 1.0 / 3.0;
-      S ns;
-      if constexpr (FINAL || sizeof(C) == sizeof(double)) {
-        cx<double> base;
-        if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) {
-          base = to_c<double>(pv);
-        } else if constexpr (KIND == K_RK4_4) {
-          const cx<double> qv = to_c<double>(av);
-          base = cx<double>{qv.r + THIRD * cr, qv.i + THIRD * ci};
-        } else {
-          base = cx<double>{cr, ci};
-        }
-        const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
-        ns = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
-      } else {
-        const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) ? to_c<C>(pv) : n.c0;
-        const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
-        ns = to_s<S>(cx<C>{base.r + (ar * f.r - ai * f.i), base.i + (ar * f.i + ai * f.r)});
-      }
-      store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
-      if constexpr (KIND == K_RK4_2) {
-        // Q = (psi + A)/3 + h/3 k2 in the storage's precision class: Q is
-        // rounded to S either way; the last update is the FP64 one above
-        if constexpr (sizeof(C) == sizeof(double)) {
-          const cx<double> pd = to_c<double>(pv);
-          const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
-          ((S*)a.acc)[o] = to_s<S>(cx<double>{(pd.r + cr) * THIRD + t1.r, (pd.i + ci) * THIRD + t1.i});
-        } else {
-          // the third is taken in FP64: a C-rounded 1/3 would scale psi by a
-          // biased factor every step (a norm drift of ~1e-7 per step in FP32)
-          const cx<C> pc = to_c<C>(pv);
-          const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
-          const double qr = ((double)pc.r + cr) * THIRD + (double)(br * f.r - bi * f.i);
-          const double qi = ((double)pc.i + ci) * THIRD + (double)(br * f.i + bi * f.r);
-          ((S*)a.acc)[o] = to_s<S>(cx<double>{qr, qi});
-        }
-      }
-      if constexpr (FINAL) {
-        if (a.want_norm) {
-          const double sr = (double)ns.x, si = (double)ns.y;
-          r_norm += (cc.wxy * a.wz[k]) * (sr * sr + si * si);
-        }
-      }
-    } else if constexpr (KIND != K_CK_6 && sizeof(C) != sizeof(double)) {
-      // Cash-Karp stages 1-5 in the stencil's compute type: K_m = dt f and
-      // tmp = psi + sum_j b_j K_j feed the next stencil only
-      const cx<C> Km{(C)a.cf_r[0] * f.r - (C)a.cf_i[0] * f.i, (C)a.cf_r[0] * f.i + (C)a.cf_i[0] * f.r};
-      const S Ks = to_s<S>(Km);
-      ((S*)a.kout)[o] = Ks;
-      const cx<C> Kmc = to_c<C>(Ks);
-      const cx<C> pc = (KIND == K_CK_1) ? n.c0 : to_c<C>(pv);
-      C tr = pc.r, ti = pc.i;
+    cx<C> dpx[PY], f[PY];
 #pragma unroll
-      for (int m = 0; m < T::NK; ++m) {
-        const cx<C> km = to_c<C>(kv[m]);
-        tr = tr + (C)a.b[m] * km.r;
-        ti = ti + (C)a.b[m] * km.i;
+    for (int q = 0; q < PY; ++q) dpx[q] = cx<C>{0, 0};
+    if (a.has_urhs) {
+#pragma unroll
+      for (int q = 0; q < PY; ++q) dpx[q] = d1<C, R>(n[q].xm2, n[q].xm1, n[q].xp1, n[q].xp2, (C)a.ix1);
+    }
+    gp_rhs_n<C, PY>(a, c0, lap, dpx, cc, k, f);
+    S* out = (S*)a.out;
+    constexpr bool FINAL = (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4 || KIND == K_CK_6);
+    S ns[PY];  // the stored stencil output of each site
+
+#pragma unroll
+    for (int q = 0; q < PY; ++q) {
+      S pv = szero<S>(), av = szero<S>();
+      {
+        int m = 0;
+        if constexpr (T::HAS_PSI) pv = pw[q][m++];
+        if constexpr (T::HAS_ACC) av = pw[q][m++];
       }
-      tr = tr + (C)a.b[T::NK] * Kmc.r;
-      ti = ti + (C)a.b[T::NK] * Kmc.i;
-      store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<C>{tr, ti}));
-    } else {
-      // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
-      const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
-      const S Ks = to_s<S>(Km);
-      const cx<double> Kmd = to_c<double>(Ks);
-      const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
-      if constexpr (KIND != K_CK_6) {
-        ((S*)a.kout)[o] = Ks;
-        double tr = pd.r, ti = pd.i;
+      constexpr int K0 = (T::HAS_PSI ? 1 : 0) + (T::HAS_ACC ? 1 : 0);
+      const double cr = (double)c0[q].r, ci = (double)c0[q].i;
+      const cx<double> fd{(double)f[q].r, (double)f[q].i};
+
+      if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 ||
+                    KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) {
+        // out = base + cf0 * f, with base = psi_n (pv), the stencil centre,
+        // or for RK4 stage 4 the accumulator plus a third of the centre.
+        // Outputs that are a new psi (Euler, RK2 stage 2, RK4 stage 4) are
+        // formed in FP64; intermediate stage inputs in the stencil's compute
+        // type C (identical to FP64 when C = double).
+        //
+        // RK4 runs in a reduced-traffic form of classical RK4 (h = dt):
+        //   s1: A = psi + h/2 k1
+        //   s2: B = psi + h/2 k2,  Q = (psi + A)/3 + h/3 k2  (= 2psi/3 + h/6 k1 + h/3 k2)
+        //   s3: A = psi + h k3
+        //   s4: psi' = Q + A/3 + h/6 k4  (= psi + h (k1/6 + k2/3 + k3/3 + k4/6))
+        // so that stage 1 reads 1 field, stage 3 reads 2 and stage 4 reads 2
+        // (solve.f90:124-148 keeps k1..k4; the sum is the same).
+        constexpr double THIRD = 1.0 / 3.0;
+        if constexpr (FINAL || sizeof(C) == sizeof(double)) {
+          cx<double> base;
+          if constexpr (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) {
+            base = to_c<double>(pv);
+          } else if constexpr (KIND == K_RK4_4) {
+            const cx<double> qv = to_c<double>(av);
+            base = cx<double>{qv.r + THIRD * cr, qv.i + THIRD * ci};
+          } else {
+            base = cx<double>{cr, ci};
+          }
+          const cx<double> t0 = cmuld(a.cf_r[0], a.cf_i[0], fd);
+          ns[q] = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
+        } else {
+          const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) ? to_c<C>(pv) : c0[q];
+          const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
+          ns[q] = to_s<S>(cx<C>{base.r + (ar * f[q].r - ai * f[q].i), base.i + (ar * f[q].i + ai * f[q].r)});
+        }
+        if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        if constexpr (KIND == K_RK4_2) {
+          // Q = (psi + A)/3 + h/3 k2 in the storage's precision class: Q is
+          // rounded to S either way; the last update is the FP64 one above.
+          // The third is taken in FP64 also for C = float: a C-rounded 1/3
+          // would scale psi by a biased factor every step.
+          S qs;
+          if constexpr (sizeof(C) == sizeof(double)) {
+            const cx<double> pd = to_c<double>(pv);
+            const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
+            qs = to_s<S>(cx<double>{(pd.r + cr) * THIRD + t1.r, (pd.i + ci) * THIRD + t1.i});
+          } else {
+            const cx<C> pc = to_c<C>(pv);
+            const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
+            const double qr = ((double)pc.r + cr) * THIRD + (double)(br * f[q].r - bi * f[q].i);
+            const double qi = ((double)pc.i + ci) * THIRD + (double)(br * f[q].i + bi * f[q].r);
+            qs = to_s<S>(cx<double>{qr, qi});
+          }
+          if (act[q]) ((S*)a.acc)[o[q]] = qs;
+        }
+      } else if constexpr (KIND != K_CK_6 && sizeof(C) != sizeof(double)) {
+        // Cash-Karp stages 1-5 in the stencil's compute type: K_m = dt f and
+        // tmp = psi + sum_j b_j K_j feed the next stencil only
+        const cx<C> Km{(C)a.cf_r[0] * f[q].r - (C)a.cf_i[0] * f[q].i,
+                       (C)a.cf_r[0] * f[q].i + (C)a.cf_i[0] * f[q].r};
+        const S Ks = to_s<S>(Km);
+        if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+        const cx<C> Kmc = to_c<C>(Ks);
+        const cx<C> pc = (KIND == K_CK_1) ? c0[q] : to_c<C>(pv);
+        C tr = pc.r, ti = pc.i;
 #pragma unroll
         for (int m = 0; m < T::NK; ++m) {
-          const cx<double> km = to_c<double>(kv[m]);
-          tr = tr + a.b[m] * km.r;
-          ti = ti + a.b[m] * km.i;
+          const cx<C> km = to_c<C>(pw[q][K0 + m]);
+          tr = tr + (C)a.b[m] * km.r;
+          ti = ti + (C)a.b[m] * km.i;
         }
-        tr = tr + a.b[T::NK] * Kmd.r;
-        ti = ti + a.b[T::NK] * Kmd.i;
-        store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, to_s<S>(cx<double>{tr, ti}));
+        tr = tr + (C)a.b[T::NK] * Kmc.r;
+        ti = ti + (C)a.b[T::NK] * Kmc.i;
+        ns[q] = to_s<S>(cx<C>{tr, ti});
+        if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
       } else {
-        // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
-        // contribute exact zeros and are skipped.
-        const cx<double> k1 = to_c<double>(kv[0]), k3 = to_c<double>(kv[1]);
-        const cx<double> k4 = to_c<double>(kv[2]), k5 = to_c<double>(kv[3]);
-        const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
-        const double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0;
-        const double DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0, DC6 = C6 - 0.25;
-        const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
-        const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
-        const S ns = to_s<S>(cx<double>{nr, ni});
-        store_at(out, g, o, i, j, k, cc.gx, cc.gy, gz, ns);
-        const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
-        const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
-        // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
-        const double fa = hypot(k1.r, k1.i) * a.inv_adt;
-        const double sr = (hypot(pd.r, pd.i) + a.dte_r * fa) + 1e-30;
-        const double si = a.dte_i * fa;
-        const double ratio = hypot(er, ei) / hypot(sr, si);
-        r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
-        if (a.want_norm) {
-          const double qr = (double)ns.x, qi = (double)ns.y;
-          r_norm += (cc.wxy * a.wz[k]) * (qr * qr + qi * qi);
+        // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
+        const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
+        const S Ks = to_s<S>(Km);
+        const cx<double> Kmd = to_c<double>(Ks);
+        const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
+        if constexpr (KIND != K_CK_6) {
+          if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+          double tr = pd.r, ti = pd.i;
+#pragma unroll
+          for (int m = 0; m < T::NK; ++m) {
+            const cx<double> km = to_c<double>(pw[q][K0 + m]);
+            tr = tr + a.b[m] * km.r;
+            ti = ti + a.b[m] * km.i;
+          }
+          tr = tr + a.b[T::NK] * Kmd.r;
+          ti = ti + a.b[T::NK] * Kmd.i;
+          ns[q] = to_s<S>(cx<double>{tr, ti});
+          if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        } else {
+          // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
+          // contribute exact zeros and are skipped.
+          const cx<double> k1 = to_c<double>(pw[q][K0]), k3 = to_c<double>(pw[q][K0 + 1]);
+          const cx<double> k4 = to_c<double>(pw[q][K0 + 2]), k5 = to_c<double>(pw[q][K0 + 3]);
+          const double C1 = 37.0 / 378.0, C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0;
+          const double DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0;
+          const double DC4 = C4 - 13525.0 / 55296.0, DC5 = 0.0 - 277.0 / 14336.0, DC6 = C6 - 0.25;
+          const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
+          const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
+          ns[q] = to_s<S>(cx<double>{nr, ni});
+          if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
+          const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
+          // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
+          const double fa = hypot(k1.r, k1.i) * a.inv_adt;
+          const double sr = (hypot(pd.r, pd.i) + a.dte_r * fa) + 1e-30;
+          const double si = a.dte_i * fa;
+          const double ratio = hypot(er, ei) / hypot(sr, si);
+          if (act[q]) r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
+        }
+      }
+    }
+    if constexpr (FINAL) {
+      if (a.want_norm) {
+        const double wz = a.wz[k];
+#pragma unroll
+        for (int q = 0; q < PY; ++q) {
+          const double sr = (double)ns[q].x, si = (double)ns[q].y;
+          const double v = (cc[q].wxy * wz) * (sr * sr + si * si);
+          if (act[q]) r_norm += v;
         }
       }
     }
   }
+}
+
+// Single-site form (one site per thread).
+template <class S, class C, int R, int KIND>
+__device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, const S* pw, int i, int j, int k,
+                                           long long o, int gz, const ColumnConsts& cc, double& r_norm,
+                                           double& r_en, double& r_err) {
+  constexpr int NPWX = StageTraits<KIND>::NPW > 0 ? StageTraits<KIND>::NPW : 1;
+  const Nb<C> nn[1] = {n};
+  S pv[1][NPWX];
+#pragma unroll
+  for (int f = 0; f < StageTraits<KIND>::NPW; ++f) pv[0][f] = pw[f];
+  const bool act[1] = {true};
+  const int jj[1] = {j};
+  const long long oo[1] = {o};
+  const ColumnConsts c1[1] = {cc};
+  sites_stage<S, C, R, KIND, 1, NPWX>(a, nn, pv, act, i, jj, k, oo, gz, c1, r_norm, r_en, r_err);
 }
 
 // ---------------------------------------------------------------------------

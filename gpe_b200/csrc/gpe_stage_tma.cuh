@@ -286,34 +286,33 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     if (okw) {
       const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
       const int gz = (k <= R || k >= g.nz - 1 - R) ? ghost_pos(k, g.nz, R, a.bcs) : NOGHOST;
+      Nb<C> n[PY];
+      S pv[PY][NPW > 0 ? NPW : 1];
 #pragma unroll
       for (int r = 0; r < PY; ++r) {
-        if (!act[r]) continue;
         const int c0 = cofs[r];
-        Nb<C> n;
-        n.c0 = to_c<C>(q[r][R]);
-        n.xm1 = to_c<C>(tile[c0 - 1]);
-        n.xp1 = to_c<C>(tile[c0 + 1]);
-        n.ym1 = to_c<C>(tile[c0 - TW]);
-        n.yp1 = to_c<C>(tile[c0 + TW]);
-        n.zm1 = to_c<C>(q[r][R - 1]);
-        n.zp1 = to_c<C>(q[r][R + 1]);
+        n[r].c0 = to_c<C>(q[r][R]);
+        n[r].xm1 = to_c<C>(tile[c0 - 1]);
+        n[r].xp1 = to_c<C>(tile[c0 + 1]);
+        n[r].ym1 = to_c<C>(tile[c0 - TW]);
+        n[r].yp1 = to_c<C>(tile[c0 + TW]);
+        n[r].zm1 = to_c<C>(q[r][R - 1]);
+        n[r].zp1 = to_c<C>(q[r][R + 1]);
         if constexpr (R == 2) {
-          n.xm2 = to_c<C>(tile[c0 - 2]);
-          n.xp2 = to_c<C>(tile[c0 + 2]);
-          n.ym2 = to_c<C>(tile[c0 - 2 * TW]);
-          n.yp2 = to_c<C>(tile[c0 + 2 * TW]);
-          n.zm2 = to_c<C>(q[r][0]);
-          n.zp2 = to_c<C>(q[r][4]);
+          n[r].xm2 = to_c<C>(tile[c0 - 2]);
+          n[r].xp2 = to_c<C>(tile[c0 + 2]);
+          n[r].ym2 = to_c<C>(tile[c0 - 2 * TW]);
+          n[r].yp2 = to_c<C>(tile[c0 + 2 * TW]);
+          n[r].zm2 = to_c<C>(q[r][0]);
+          n[r].zp2 = to_c<C>(q[r][4]);
         } else {
-          n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
+          n[r].xm2 = n[r].xp2 = n[r].ym2 = n[r].yp2 = n[r].zm2 = n[r].zp2 = cx<C>{0, 0};
         }
-        S pv[NPW > 0 ? NPW : 1];
         const int pofs = (tyt + r * TYT) * TX + tx;
 #pragma unroll
-        for (int f = 0; f < NPW; ++f) pv[f] = pws[f * (TX * TY) + pofs];
-        site_stage<S, C, R, KIND>(a, n, pv, i, jr[r], k, o[r], gz, cc[r], r_norm, r_en, r_err);
+        for (int f = 0; f < NPW; ++f) pv[r][f] = pws[f * (TX * TY) + pofs];
       }
+      sites_stage<S, C, R, KIND, PY>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err);
     }
 #pragma unroll
     for (int r = 0; r < PY; ++r) {
