@@ -83,6 +83,12 @@ class GpeResult(C.Structure):
     ]
 
 
+class GpeCondensedInfo(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("M", "n0", "rho0", "tot", "temp", "temp2", "H", "mass_density")]
+
+
+GPE_SPECTRUM_SHELLS = 7
+
 _PROTOS = {
     "gpe_create": (C.c_int, [C.POINTER(GpeParams), C.POINTER(C.c_void_p)]),
     "gpe_destroy": (None, [C.c_void_p]),
@@ -110,6 +116,9 @@ _PROTOS = {
     "gpe_pool_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeParams), C.POINTER(GpeIC), C.c_int64, C.c_uint64,
                                      C.c_void_p]),
     "gpe_set_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeIC)]),
+    "gpe_condensed": (C.c_int, [C.c_void_p, C.POINTER(GpeCondensedInfo), C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_int32]),
+    "gpe_filtered": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_int32]),
     "gpe_pool_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
     "gpe_pool_poll": (C.c_int, [C.c_void_p, C.POINTER(GpeResult), C.c_int32, C.POINTER(C.c_int32)]),
     "gpe_pool_free_bytes": (C.c_int64, [C.c_void_p]),

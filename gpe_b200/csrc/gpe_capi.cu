@@ -21,6 +21,7 @@
 #include "gpe_device.cuh"
 #include "gpe_stage_tma.cuh"
 #include "gpe_common.h"
+#include "gpe_fft.h"
 #include "gpe_ic.h"
 
 namespace gpe {
@@ -83,6 +84,10 @@ struct gpe_handle {
   int tma_ty = 4;  // threads per CTA in y for the 32 x 8 tile: 4 = two rows per thread, 8 = one
   std::vector<CUtensorMap> map_halo, map_pw;  // per field
   int* status = nullptr;                      // device status word
+  // FFT diagnostics: transform scratch + the reference's k-grid symbols
+  void* fft_work = nullptr;
+  size_t fft_work_bytes = 0;
+  double* fft_kq = nullptr;
 };
 
 namespace {
@@ -553,6 +558,7 @@ void gpe_destroy(gpe_handle* h) {
   if (h->hres) cudaFreeHost(h->hres);
   if (h->staging) cudaFree(h->staging);
   if (h->status) cudaFree(h->status);
+  if (h->fft_work) cudaFree(h->fft_work);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -689,6 +695,85 @@ int gpe_energy(gpe_handle* h, double* energy) {
   if (int rc = finalize_into(h, h->part_a, 0)) return rc;
   if (int rc = fetch_results(h)) return rc;
   *energy = ((h->hres[1] * h->dx) * h->dy) * h->dz;
+  return GPE_OK;
+}
+
+// FFT scratch on first use: transform buffer + partials, then the k tables
+static int ensure_fft(gpe_handle* h) {
+  if (h->fft_work) return GPE_OK;
+  const size_t need = fft_work_bytes(h->p);
+  const int nk = h->p.nx + h->p.ny + h->p.nz;
+  if (cudaMalloc(&h->fft_work, need + nk * sizeof(double)) != cudaSuccess) {
+    h->fft_work = nullptr;
+    return fail(h, GPE_ERR_NOMEM, "cudaMalloc failed for the FFT diagnostics scratch");
+  }
+  h->fft_work_bytes = need;
+  h->fft_kq = (double*)((char*)h->fft_work + need);
+  std::vector<double> kq(nk);
+  fft_kq_axis(h->p.nx, h->p.nx, h->dx, kq.data());
+  fft_kq_axis(h->p.ny, h->p.nx, h->dy, kq.data() + h->p.nx);
+  fft_kq_axis(h->p.nz, h->p.nx, h->dz, kq.data() + h->p.nx + h->p.ny);
+  CU(h, cudaMemcpy(h->fft_kq, kq.data(), nk * sizeof(double), cudaMemcpyHostToDevice));
+  return GPE_OK;
+}
+
+int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t* nharm, double* F, int32_t nF) {
+  if (!h || !info) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (F && nF != h->p.nx / 2) return fail(h, GPE_ERR_BADARG, "gpe_condensed: nF must be nx/2");
+  CU(h, cudaSetDevice(h->dev));
+  if (int rc = ensure_fft(h)) return rc;
+  const bool spec = eta || nharm || F;
+  FftDiag d;
+  CU(h, fft_condensed(h->p, h->g, h->esz, h->fields[h->cur], h->fft_kq, spec, h->fft_work, h->fft_work_bytes,
+                      h->st, d));
+  // io.f90:331-381, in the reference's expression order
+  const double V = (double)h->p.nx * (double)h->p.ny * (double)h->p.nz;
+  const long long Vi = (long long)h->p.nx * h->p.ny * h->p.nz;
+  const double M = ((d.mass_sum * h->dx) * h->dy) * h->dz;
+  const double vol8 = ((8.0 * h->p.xr) * h->p.yr) * h->p.zr;
+  info->M = M;
+  info->n0 = d.n0;
+  info->rho0 = d.n0 / V;
+  info->tot = d.tot;
+  info->temp = (M - d.n0) / d.tot;
+  const double E0 = (1.0 / (double)(2 * Vi)) * (M * M + (M - d.n0) * (M - d.n0));
+  info->H = E0 + info->temp * (double)(Vi - 1);
+  info->temp2 = ((M / vol8) - (d.n0 / V)) / d.tot;
+  info->mass_density = M / vol8;
+  for (int m = 0; m < GPE_SPECTRUM_SHELLS; ++m) {
+    const double e = d.eta[m];
+    const double c = d.nharm[m];
+    if (nharm) nharm[m] = (int32_t)c;
+    if (eta) eta[m] = (e == 0.0) ? e : e / c;
+  }
+  if (F) {
+    double acc = 0.0;
+    for (int kk = 1; kk <= nF; ++kk) {
+      acc += d.H[kk];
+      F[kk - 1] = acc;
+    }
+  }
+  return GPE_OK;
+}
+
+int gpe_filtered(gpe_handle* h, double m, double filter_kc, void* out, int32_t dtype) {
+  if (!h || !out) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (!(filter_kc > 0.0)) return fail(h, GPE_ERR_BADARG, "gpe_filtered: filter_kc must be > 0");
+  if (dtype != GPE_C128 && dtype != GPE_C64) return fail(h, GPE_ERR_BADARG, "gpe_filtered: bad dtype");
+  CU(h, cudaSetDevice(h->dev));
+  if (int rc = ensure_fft(h)) return rc;
+  CU(h, fft_filtered(h->p, h->g, h->esz, h->fields[h->cur], m, filter_kc, h->fft_work, h->fft_work_bytes, h->st));
+  const size_t n = (size_t)h->p.nx * h->p.ny * h->p.nz;
+  if (dtype == GPE_C128) {
+    CU(h, cudaMemcpyAsync(out, h->fft_work, n * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+  } else {
+    std::vector<double2> tmp(n);
+    CU(h, cudaMemcpyAsync(tmp.data(), h->fft_work, n * sizeof(double2), cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+    float2* o = (float2*)out;
+    for (size_t t = 0; t < n; ++t) o[t] = make_float2((float)tmp[t].x, (float)tmp[t].y);
+  }
   return GPE_OK;
 }
 

@@ -207,9 +207,11 @@ __global__ void k_pack_scaled(const double2* __restrict__ buf, const double* __r
   }
 }
 
-// inverse 3-D Z2Z plans, one per (device, grid), created on first use
+// 3-D Z2Z plans, one per (device, grid), created on first use
 std::mutex g_plan_mu;
 std::map<std::tuple<int, int, int, int>, cufftHandle> g_plans;
+
+}  // namespace
 
 bool plan_for(int nx, int ny, int nz, cufftHandle* out) {
   int dev = 0;
@@ -227,8 +229,6 @@ bool plan_for(int nx, int ny, int nz, cufftHandle* out) {
   *out = p;
   return true;
 }
-
-}  // namespace
 
 int ic_validate(const gpe_ic* ic, std::string& why) {
   if (!ic || ic->nfactors < 1 || ic->nfactors > 4) {

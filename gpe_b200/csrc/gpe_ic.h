@@ -1,6 +1,7 @@
 // Device initial conditions shared by the handle and the pool.
 #pragma once
 #include <cuda_runtime.h>
+#include <cufft.h>
 
 #include <string>
 
@@ -16,5 +17,8 @@ size_t ic_work_bytes(const gpe_params& p, const gpe_ic& ic);
 // write the initial state (with ghosts) into psi_field on stream st
 cudaError_t ic_generate(const gpe_params& p, const Geom& g, int esz, int R, const gpe_ic& ic, void* psi_field,
                         void* work, size_t work_bytes, cudaStream_t st);
+
+// cached 3-D Z2Z cuFFT plan for an (nz, ny, nx) grid on the current device
+bool plan_for(int nx, int ny, int nz, cufftHandle* out);
 
 }  // namespace gpe

@@ -180,6 +180,33 @@ class Solver:
         _check(self.lib, self.h, self.lib.gpe_energy(self.h, C.byref(v)))
         return v.value
 
+    def condensed(self, spectrum: bool = False):
+        """condensed_particles (src/io.f90:304-395) of the current state on the
+        device: a dict with the mass.dat quantities and, with spectrum=True,
+        eta/nharm (7 shells) and F (kk = 1..nx/2) of src/io.f90:668-714."""
+        info = L.GpeCondensedInfo()
+        if spectrum:
+            eta = np.zeros(L.GPE_SPECTRUM_SHELLS)
+            nharm = np.zeros(L.GPE_SPECTRUM_SHELLS, dtype=np.int32)
+            F = np.zeros(self.params.nx // 2)
+            rc = self.lib.gpe_condensed(self.h, C.byref(info), eta.ctypes.data, nharm.ctypes.data, F.ctypes.data,
+                                        len(F))
+        else:
+            rc = self.lib.gpe_condensed(self.h, C.byref(info), None, None, None, 0)
+        _check(self.lib, self.h, rc)
+        out = {n: getattr(info, n) for n, _ in L.GpeCondensedInfo._fields_}
+        if spectrum:
+            out.update(eta=eta, nharm=nharm, F=F)
+        return out
+
+    def filtered(self, filter_kc: float, m: float = 1.0, dtype=np.complex128) -> np.ndarray:
+        """filtered_surface's low-passed field (src/io.f90:524-571), (nz, ny, nx)."""
+        p = self.params
+        out = np.empty((p.nz, p.ny, p.nx), dtype=dtype)
+        code = L.GPE_C128 if out.dtype == np.complex128 else L.GPE_C64
+        _check(self.lib, self.h, self.lib.gpe_filtered(self.h, float(m), float(filter_kc), out.ctypes.data, code))
+        return out
+
     def renormalise(self, norm: float) -> None:
         _check(self.lib, self.h, self.lib.gpe_renormalise(self.h, float(norm)))
 

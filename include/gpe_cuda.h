@@ -187,6 +187,40 @@ typedef struct {
 /* Set the handle's state to the initial condition (no host array). */
 int gpe_set_ic(gpe_handle* h, const gpe_ic* ic);
 
+/* FFT diagnostics of the current state, computed on the device in FP64
+ * (cuFFT), with the reference's transform a = DFT(psi)/sqrt(nx ny nz)
+ * (src/ic.f90:910-939).
+ *
+ * gpe_condensed replaces condensed_particles (src/io.f90:304-395): the
+ * record of mass.dat plus, when eta/nharm/F are non-NULL, the spectra of
+ * spectrum (src/io.f90:668-714): the mean occupation eta[m] of the 7 shells
+ * m-1 <= |log2(|k|/2pi)| < m (already divided by the shell's site count
+ * nharm[m], as written to spectrum/spectrum<p>.dat) and the integral
+ * distribution F[kk-1] = sum over 0 < |k| <= kk of |a|^2, kk = 1..nF, with
+ * nF = nx/2 (idf/idf<p>.dat).  |k| is the integer index distance of the
+ * reference.  Sums are deterministic (fixed order on the device). */
+typedef struct {
+  double M;        /* mass: sum |psi|^2 dx dy dz (src/variables.f90:608-628)   */
+  double n0;       /* |a(0,0,0)|^2                                             */
+  double rho0;     /* n0 / (nx ny nz)                                          */
+  double tot;      /* sum (k2 + rho0)/(k2^2 + 2 rho0 k2) (src/io.f90:343-360)  */
+  double temp;     /* (M - n0)/tot                                             */
+  double temp2;    /* (M/(8 xr yr zr) - n0/V)/tot                              */
+  double H;        /* E0 + temp (V - 1), E0 = (M^2 + (M - n0)^2)/(2V)          */
+  double mass_density; /* M/(8 xr yr zr), column 3 of mass.dat                */
+} gpe_condensed_info;
+
+#define GPE_SPECTRUM_SHELLS 7
+
+int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t* nharm, double* F, int32_t nF);
+
+/* filtered_surface (src/io.f90:524-571): the state low-passed in spectral
+ * space, a -> a max(1 - m k2 / filter_kc^2, 0), transformed back; written to
+ * the host buffer out (nx*ny*nz complex, x fastest, dtype GPE_C128 or
+ * GPE_C64).  m = 1 for the reference's periodic saves, fscale * ind in
+ * post-processing (src/io.f90:540-544). */
+int gpe_filtered(gpe_handle* h, double m, double filter_kc, void* out, int32_t dtype);
+
 /* Stage-kernel kinds reported by gpe_profile_get (one fused kernel each). */
 #define GPE_KIND_EULER 0
 #define GPE_KIND_RK2_1 1
