@@ -119,6 +119,7 @@ _PROTOS = {
     "gpe_condensed": (C.c_int, [C.c_void_p, C.POINTER(GpeCondensedInfo), C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_int32]),
     "gpe_filtered": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_int32]),
+    "gpe_get_site": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "gpe_pool_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
     "gpe_pool_poll": (C.c_int, [C.c_void_p, C.POINTER(GpeResult), C.c_int32, C.POINTER(C.c_int32)]),
     "gpe_pool_free_bytes": (C.c_int64, [C.c_void_p]),

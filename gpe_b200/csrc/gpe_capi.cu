@@ -814,6 +814,26 @@ int gpe_get_grid(const gpe_handle* h, double* x, double* y, double* z, double* d
   return GPE_OK;
 }
 
+int gpe_get_site(gpe_handle* h, int32_t i, int32_t j, int32_t k, double* re_im) {
+  if (!h || !re_im) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (i < 0 || i >= h->p.nx || j < 0 || j >= h->p.ny || k < 0 || k >= h->p.nz)
+    return fail(h, GPE_ERR_BADARG, "gpe_get_site: index outside the grid");
+  CU(h, cudaSetDevice(h->dev));
+  const long long o = (long long)(k + 2) * h->g.pz + (long long)(j + 2) * h->g.px + h->g.xoff + i;
+  const char* src = (const char*)h->fields[h->cur] + o * h->esz;
+  if (h->esz == 16) {
+    CU(h, cudaMemcpyAsync(re_im, src, 16, cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+  } else {
+    float v[2];
+    CU(h, cudaMemcpyAsync(v, src, 8, cudaMemcpyDeviceToHost, h->st));
+    CU(h, cudaStreamSynchronize(h->st));
+    re_im[0] = v[0];
+    re_im[1] = v[1];
+  }
+  return GPE_OK;
+}
+
 int gpe_get_stream(const gpe_handle* h, void** stream) {
   if (!h || !stream) return GPE_ERR_BADARG;
   *stream = (void*)h->st;

@@ -11,10 +11,13 @@
 //                  vr1 = ring_param(...) (src/parameters.in:22-70)
 //   ic.in          the active "init_cond = ..." product (src/ic.in), built on
 //                  the device by gpe_set_ic
-// Outputs: norm.dat, energy.dat, timestep.dat (Fortran e17.9 records, as
-// src/io.f90:188-207, 399-413 and src/solve.f90:234-241), proc0000/
-// end_state.dat + save.dat (src/io.f90:831-882), proc0000/dens<p>.dat and
-// p_saved.dat when save_3d (src/io.f90:480-520).  Control files: RUNNING
+// Outputs: norm.dat, energy.dat, psi_time.dat, mass.dat, timestep.dat
+// (Fortran e17.9 records, as src/io.f90:136-207, 304-381, 399-413 and
+// src/solve.f90:234-241), proc0000/end_state.dat + save.dat
+// (src/io.f90:831-882), proc0000/dens<p>.dat and p_saved.dat when save_3d
+// (src/io.f90:480-520), spectrum/, idf/ and eta_time.dat when save_spectrum
+// (src/io.f90:623-716), proc0000/filtered<p>.dat when save_filter
+// (src/io.f90:524-620); <p> is itos(p), seven zero-padded digits.  Control files: RUNNING
 // (delete to stop), SAVE (write a 3-D snapshot), ERROR (written on a fatal
 // error, as src/error.f90:24-46).  Restart reads end_state0000.dat
 // (src/ic.f90:117-191).
@@ -160,7 +163,8 @@ struct RunIn {
   double Urhs = 0, diss_amp = 0, scal = 1, nv = 0, enerv = 0, g = 1, mu = 1, nn = 1, omx = 0, omy = 0, omz = 0;
   int save_rate = 10;
   double save_rate2 = 1e300, save_rate3 = 1e300, p_save = 1e300;
-  bool save_3d = false;
+  bool save_3d = false, save_spectrum = false, save_filter = false;
+  double filter_kc = 10.0;
 };
 
 RunIn parse_run_in() {
@@ -213,6 +217,9 @@ RunIn parse_run_in() {
   num(io, "save_rate3", r.save_rate3);
   num(io, "p_save", r.p_save);
   lg(io, "save_3d", r.save_3d);
+  lg(io, "save_spectrum", r.save_spectrum);
+  lg(io, "save_filter", r.save_filter);
+  num(io, "filter_kc", r.filter_kc);
   return r;
 }
 
@@ -482,10 +489,21 @@ void state_restart(Ctx& c) {
   check(c, gpe_set_state(c.h, b.data(), c.esz == 16 ? GPE_C128 : GPE_C64));
 }
 
-// idl_surface (src/io.f90:480-520): proc0000/dens<p>.dat + p_saved.dat
+// itos (src/io.f90:29-47): the last seven digits of n, zero-padded
+std::string itos(int64_t n) {
+  char d[8];
+  for (int i = 6; i >= 0; --i) {
+    d[i] = (char)('0' + (int)(n % 10));
+    n /= 10;
+  }
+  d[7] = 0;
+  return d;
+}
+
+// idl_surface (src/io.f90:480-520): proc0000/dens<itos(p)>.dat + p_saved.dat
 void idl_surface(Ctx& c) {
   mkdir(path("proc0000").c_str(), 0755);
-  const std::string name = "proc0000/dens" + std::to_string(c.p) + ".dat";
+  const std::string name = "proc0000/dens" + itos(c.p) + ".dat";
   FILE* f = fopen(path(name).c_str(), "wb");
   if (!f) emergency_stop("ERROR: cannot write " + name);
   wr_real(f, c, c.t + c.im_t);
@@ -502,6 +520,69 @@ void idl_surface(Ctx& c) {
 }
 
 double fmodulo(double a, double b) { return a - std::floor(a / b) * b; }
+
+std::string fi(long long v, int w) {
+  char b[32];
+  snprintf(b, sizeof b, "%*lld", w, v);
+  return b;
+}
+
+// save_time (src/io.f90:136-184): psi, |psi|^2 and its phase at the centre
+// site into psi_time.dat
+void save_time(Ctx& c, double time) {
+  double v[2];
+  check(c, gpe_get_site(c.h, c.P.nx / 2, c.P.ny / 2, c.P.nz / 2, v));
+  const double h = std::hypot(v[0], v[1]);
+  const double phase = std::atan2(v[1] + 1.0e-6, v[0]);  // get_phase (src/variables.f90:379-391)
+  append_line("psi_time.dat", fe(time) + fe(c.im_t) + fe(v[0]) + fe(v[1]) + fe(h * h) + fe(phase));
+}
+
+// condensed_particles (src/io.f90:304-395) with spectrum (io.f90:623-716)
+// and filtered_surface(a, 0) (io.f90:524-620), all on the device
+void condensed_particles(Ctx& c, double time) {
+  const int nF = c.P.nx / 2;
+  const bool spec = c.r.save_spectrum;
+  gpe_condensed_info d;
+  std::vector<double> eta(GPE_SPECTRUM_SHELLS), F(nF);
+  std::vector<int32_t> nh(GPE_SPECTRUM_SHELLS);
+  check(c, gpe_condensed(c.h, &d, spec ? eta.data() : nullptr, spec ? nh.data() : nullptr,
+                         spec ? F.data() : nullptr, spec ? nF : 0));
+  const double V = (double)c.P.nx * c.P.ny * c.P.nz;
+  append_line("mass.dat", fe(time) + fe(c.im_t) + fe(d.mass_density) + fe(d.n0 / V) + fe(d.M) + fe(d.n0) +
+                              fe(d.temp) + fe(d.temp2) + fe(d.H / V));
+  if (spec) {
+    mkdir(path("spectrum").c_str(), 0755);
+    mkdir(path("idf").c_str(), 0755);
+    std::string body;
+    for (int m = 0; m < GPE_SPECTRUM_SHELLS; ++m) body += fi(m + 1, 9) + fi(nh[m], 9) + fe(eta[m]) + "\n";
+    FILE* f = fopen(path("spectrum/spectrum" + itos(c.p) + ".dat").c_str(), "w");
+    if (!f) emergency_stop("ERROR: cannot write spectrum/spectrum" + itos(c.p) + ".dat");
+    fputs(body.c_str(), f);
+    fclose(f);
+    body.clear();
+    for (int kk = 1; kk <= nF; ++kk) body += fi(kk, 9) + fe(F[kk - 1]) + "\n";
+    f = fopen(path("idf/idf" + itos(c.p) + ".dat").c_str(), "w");
+    if (!f) emergency_stop("ERROR: cannot write idf/idf" + itos(c.p) + ".dat");
+    fputs(body.c_str(), f);
+    fclose(f);
+    append_line("eta_time.dat", fe(c.t) + fe(eta[0]) + fe(eta[1]) + fe(eta[2]));
+  }
+  if (c.r.save_filter) {
+    mkdir(path("proc0000").c_str(), 0755);
+    const std::string name = "proc0000/filtered" + itos(c.p) + ".dat";
+    std::vector<char> b((size_t)c.P.nx * c.P.ny * c.P.nz * c.esz);
+    check(c, gpe_filtered(c.h, 1.0, c.r.filter_kc, b.data(), c.esz == 16 ? GPE_C128 : GPE_C64));
+    FILE* f = fopen(path(name).c_str(), "wb");
+    if (!f) emergency_stop("ERROR: cannot write " + name);
+    wr_real(f, c, c.t);
+    for (int v : {c.P.nx, c.P.ny, c.P.nz, 1, 1, 0, c.P.ny - 1, 0, c.P.nz - 1}) wr_int(f, v);
+    fwrite(b.data(), 1, b.size(), f);
+    for (double v : c.x) wr_real(f, c, v);
+    for (double v : c.y) wr_real(f, c, v);
+    for (double v : c.z) wr_real(f, c, v);
+    fclose(f);
+  }
+}
 
 }  // namespace
 
@@ -573,8 +654,10 @@ int main(int argc, char** argv) {
     if (c.r.renorm) check(c, gpe_renormalise(c.h, prev_norm));
     append_line("norm.dat", fe(c.t) + fe(c.im_t) + fe(prev_norm) + fe(relnorm));
   }
+  condensed_particles(c, c.t);  // src/gpe.f90:116
   const double nsites = (double)p.nx * p.ny * p.nz;
   int64_t ps = (int64_t)(c.t / c.r.p_save), n2 = (int64_t)(c.t / c.r.save_rate2);
+  int64_t m3 = (int64_t)(c.t / c.r.save_rate3);
   while (c.t + c.im_t <= c.r.end_time) {
     if (!exists("RUNNING")) {  // src/gpe.f90:137-161
       printf("\n Stop requested.\n");
@@ -586,6 +669,11 @@ int main(int argc, char** argv) {
       double E = 0;
       check(c, gpe_energy(c.h, &E));
       append_line("energy.dat", fe(c.t) + fe(c.im_t) + fe(E / nsites));
+      save_time(c, c.t);
+    }
+    if (c.t + c.im_t >= c.r.save_rate3 * m3) {  // src/gpe.f90:189-198
+      condensed_particles(c, c.t);
+      ++m3;
     }
     if (c.t + c.im_t >= c.r.save_rate2 * n2) {
       if (c.r.save_3d) idl_surface(c);
@@ -630,6 +718,8 @@ int main(int argc, char** argv) {
         c.im_t = 0.0;
         ps = (int64_t)(c.t / c.r.p_save);
         n2 = (int64_t)(c.t / c.r.save_rate2);
+        m3 = (int64_t)(c.t / c.r.save_rate3);
+        if (c.r.save_3d) idl_surface(c);
         c.dt = std::complex<double>(std::fabs(c.dt.imag()), std::fabs(c.dt.real()));
         printf(" Switching to real time\n");
       }

@@ -221,6 +221,10 @@ int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t*
  * post-processing (src/io.f90:540-544). */
 int gpe_filtered(gpe_handle* h, double m, double filter_kc, void* out, int32_t dtype);
 
+/* One site of the current state, (re, im) in FP64: the probe of save_time
+ * (src/io.f90:136-184, psi at (nx/2, ny/2, nz/2) into psi_time.dat). */
+int gpe_get_site(gpe_handle* h, int32_t i, int32_t j, int32_t k, double* re_im);
+
 /* Stage-kernel kinds reported by gpe_profile_get (one fused kernel each). */
 #define GPE_KIND_EULER 0
 #define GPE_KIND_RK2_1 1

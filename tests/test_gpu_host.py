@@ -80,3 +80,61 @@ def test_host_rejects_existing_end_state(gpu, tmp_path):
     r = subprocess.run([str(HOST), "--dir", str(d)], capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
     assert "restart=.false. but end_state0000.dat exists" in (d / "ERROR").read_text()
+
+
+def test_host_diagnostics_outputs(gpu, tmp_path):
+    """mass.dat (condensed_particles), spectrum/idf/eta_time (spectrum),
+    filtered<p>.dat (filtered_surface), psi_time.dat (save_time) and
+    dens<p>.dat with the reference's itos file numbering."""
+    from oracle import fft_diag as D
+
+    d = tmp_path / "run"
+    shutil.copytree(INPUTS / "ring64", d)
+    t_in = (d / "run.in").read_text()
+    t_in = t_in.replace("save_rate3    = 100.0", "save_rate3    = 0.05")
+    t_in = t_in.replace("save_3d       = .false.",
+                        "save_3d       = .true.\n  save_spectrum = .true.\n  save_filter   = .true.\n"
+                        "  filter_kc     = 8.0")
+    (d / "run.in").write_text(t_in)
+    run(d)
+    mass = (d / "mass.dat").read_text().splitlines()
+    # at start (gpe.f90:116), first loop pass (t >= 0) and t >= 0.05; e17.9
+    # records keep 9 significant digits (relative rounding up to 5e-9)
+    assert len(mass) >= 3 and all(len(x) == 9 * 17 for x in mass)
+    psi0 = ic.vortex_ring(RP, "xy", r0=4.0)
+    rec, a = D.condensed_particles(psi0, RP.xr, RP.yr, RP.zr)
+    first = [float(v) for v in mass[0].split()]
+    V = RP.nx * RP.ny * RP.nz
+    expect = [0.0, 0.0, rec["mass_density"], rec["n0"] / V, rec["M"], rec["n0"], rec["temp"], rec["temp2"],
+              rec["H"] / V]
+    for got, want in zip(first, expect):
+        assert got == pytest.approx(want, rel=6e-9, abs=1e-300)
+    spec = (d / "spectrum" / "spectrum0000000.dat").read_text().splitlines()
+    eta, nharm, F = D.spectrum(a)
+    assert len(spec) == 7 and all(len(x) == 35 for x in spec)
+    for m, line in enumerate(spec):
+        assert int(line[:9]) == m + 1 and int(line[9:18]) == nharm[m]
+        # the device IC equals the host IC to ~1e-13, which is not small
+        # relative to the near-empty high shells: absolute scale for those
+        assert float(line[18:]) == pytest.approx(eta[m], rel=6e-9, abs=1e-11 * np.max(eta))
+    idf = (d / "idf" / "idf0000000.dat").read_text().splitlines()
+    assert len(idf) == RP.nx // 2
+    assert [float(x[9:]) for x in idf] == pytest.approx(list(F), rel=6e-9, abs=1e-11 * F[-1])
+    eta_t = (d / "eta_time.dat").read_text().splitlines()
+    assert len(eta_t) == len(mass) and all(len(x) == 4 * 17 for x in eta_t)
+    # filtered_surface stream file of the initial state
+    b = (d / "proc0000" / "filtered0000000.dat").read_bytes()
+    n = V
+    assert len(b) == 8 + 9 * 4 + 16 * n + 8 * (RP.nx + RP.ny + RP.nz)
+    filt = np.frombuffer(b[44:44 + 16 * n], dtype=np.complex128).reshape(RP.nz, RP.ny, RP.nx)
+    ref = D.filtered_surface(a, 1.0, 8.0)
+    assert np.linalg.norm(filt - ref) / np.linalg.norm(ref) <= 1e-12
+    assert (d / "proc0000" / "dens0000000.dat").exists()
+    pt = (d / "psi_time.dat").read_text().splitlines()
+    assert len(pt) >= 2 and all(len(x) == 6 * 17 for x in pt)
+    c = psi0[RP.nz // 2, RP.ny // 2, RP.nx // 2]
+    v = [float(x) for x in pt[0].split()]
+    assert v[2] == pytest.approx(c.real, rel=1e-8, abs=1e-12)
+    assert v[3] == pytest.approx(c.imag, rel=1e-8, abs=1e-12)
+    assert v[4] == pytest.approx(abs(c) ** 2, rel=1e-8, abs=1e-12)
+    assert v[5] == pytest.approx(np.arctan2(c.imag + 1e-6, c.real), rel=1e-8, abs=1e-12)
