@@ -120,6 +120,14 @@ _PROTOS = {
                                 C.c_int32]),
     "gpe_filtered": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_int32]),
     "gpe_get_site": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "gpe_slab_nccl_id": (C.c_int, [C.c_void_p]),
+    "gpe_slab_hub_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "gpe_slab_hub_destroy": (None, [C.c_void_p]),
+    "gpe_create_slab": (C.c_int, [C.POINTER(GpeParams), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                  C.POINTER(C.c_void_p)]),
+    "gpe_slab_extent": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "gpe_slab_partition": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32)]),
     "gpe_pool_step": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
     "gpe_pool_poll": (C.c_int, [C.c_void_p, C.POINTER(GpeResult), C.c_int32, C.POINTER(C.c_int32)]),
     "gpe_pool_free_bytes": (C.c_int64, [C.c_void_p]),

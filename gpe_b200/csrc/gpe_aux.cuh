@@ -9,7 +9,7 @@ namespace gpe {
 // contiguous interior (complex T2, [k][j][i]) -> ghost-padded field S with
 // its face ghosts (the halo exchange of gpe.f90:173-176, done once)
 template <class S, class T2>
-__global__ void k_pack(const T2* __restrict__ src, S* __restrict__ dst, Geom g, int R, int bcs) {
+__global__ void k_pack(const T2* __restrict__ src, S* __restrict__ dst, Geom g, int R, int bcs, int zmask = 3) {
   const long long n = (long long)g.nx * g.ny * g.nz;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t % g.nx);
@@ -22,7 +22,7 @@ __global__ void k_pack(const T2* __restrict__ src, S* __restrict__ dst, Geom g, 
     s.y = (typename Stor<S>::R)v.y;
     const long long col = (long long)(j + 2) * g.px + g.xoff + i;
     store_with_ghosts(dst, g, col, i, j, k, ghost_pos(i, g.nx, R, bcs), ghost_pos(j, g.ny, R, bcs),
-                      ghost_pos(k, g.nz, R, bcs), s);
+                      zghost_pos(k, g.nz, R, bcs, zmask), s);
   }
 }
 

@@ -23,6 +23,7 @@
 #include "gpe_common.h"
 #include "gpe_fft.h"
 #include "gpe_ic.h"
+#include "gpe_slab.h"
 
 namespace gpe {
 cudaError_t launch_stage_f64(int kind, int R, int ty, dim3 grid, cudaStream_t st, const StageArgs& a);
@@ -88,15 +89,39 @@ struct gpe_handle {
   void* fft_work = nullptr;
   size_t fft_work_bytes = 0;
   double* fft_kq = nullptr;
+  // z-slab decomposition (gpe_create_slab): this handle owns planes
+  // [k0, k0 + p.nz) of a grid of nz_global planes and exchanges R boundary
+  // planes with slab_down / slab_up (-1 = a global face) after every stage
+  int rank = 0, nranks = 1, k0 = 0, nz_global = 0;
+  int slab_down = -1, slab_up = -1;
+  bool slab = false;
+  int zghost = 3;          // z ghosts the stage kernels write (StageArgs::zghost)
+  void* nccl = nullptr;    // ncclComm_t of the NCCL transport
+  gpe::SlabHub* hub = nullptr;
+  bool own_stream = true;
+  std::string xerr;        // detail of a failed exchange, appended to the next error
+};
+
+struct gpe_slab_hub {
+  gpe::SlabHub hub;
 };
 
 namespace {
 
 int fail(gpe_handle* h, int code, const std::string& msg) {
-  if (h) h->err = msg;
-  else g_create_err = msg;
+  if (h) {
+    h->err = msg;
+    if (!h->xerr.empty()) {
+      h->err += " (" + h->xerr + ")";
+      h->xerr.clear();
+    }
+  } else {
+    g_create_err = msg;
+  }
   return code;
 }
+
+
 
 #define CU(h, call)                                                                        \
   do {                                                                                     \
@@ -156,7 +181,60 @@ cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a_in) {
   }
 }
 
+// Halo exchange of field f of a z-slab handle: the R planes next to each
+// face go to the neighbour slab's ghost planes (the role of send_recv_z,
+// src/variables.f90:203-256).  Planes are contiguous (pz elements each).
+cudaError_t slab_exchange(gpe_handle* h, int f) {
+  if (!h->slab || f < 0) return cudaSuccess;
+  const size_t plane = (size_t)h->g.pz * h->esz;
+  const int R = h->R, nzl = h->p.nz;
+  const size_t bytes = (size_t)R * plane;
+  char* base = (char*)h->fields[f];
+  char* lo_send = base + 2 * plane;                    // k = 0 .. R-1
+  char* hi_send = base + (size_t)(nzl + 2 - R) * plane;  // k = nzl-R .. nzl-1
+  char* lo_recv = base + (size_t)(2 - R) * plane;      // k = -R .. -1
+  char* hi_recv = base + (size_t)(nzl + 2) * plane;    // k = nzl .. nzl+R-1
+  if (h->nccl) {
+    // sends to down/up, then receives from up/down: with down == up (two
+    // ranks, or one rank on a periodic axis) the pairs match in this order
+    const NcclXfer xs[4] = {{h->slab_down, lo_send, nullptr, bytes},
+                            {h->slab_up, hi_send, nullptr, bytes},
+                            {h->slab_up, nullptr, hi_recv, bytes},
+                            {h->slab_down, nullptr, lo_recv, bytes}};
+    if (nccl_exchange(h->nccl, xs, 4, h->st, h->xerr) != 0) return cudaErrorUnknown;
+    return cudaSuccess;
+  }
+  SlabHub* hub = h->hub;
+  if (!hub->barrier(hub->timeout_s)) {
+    h->xerr = "a z-slab of the hub stopped calling in (barrier timeout)";
+    return cudaErrorTimeout;
+  }
+  if (h->slab_up >= 0) {
+    const gpe_handle* u = hub->slabs[h->slab_up];
+    cudaError_t e = cudaMemcpyAsync(hi_recv, (const char*)u->fields[f] + 2 * plane, bytes,
+                                    cudaMemcpyDeviceToDevice, h->st);
+    if (e != cudaSuccess) return e;
+  }
+  if (h->slab_down >= 0) {
+    const gpe_handle* d = hub->slabs[h->slab_down];
+    cudaError_t e = cudaMemcpyAsync(lo_recv, (const char*)d->fields[f] + (size_t)(d->p.nz + 2 - R) * plane, bytes,
+                                    cudaMemcpyDeviceToDevice, h->st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_prof(gpe_handle* h, int kind, const StageArgs& a);
+
+// A stage launch; on a z-slab handle its output's boundary planes are
+// exchanged before anything reads them.
 cudaError_t launch(gpe_handle* h, int kind, const StageArgs& a) {
+  cudaError_t e = launch_prof(h, kind, a);
+  if (e != cudaSuccess || !h->slab || !a.out) return e;
+  return slab_exchange(h, field_of(h, a.out));
+}
+
+cudaError_t launch_prof(gpe_handle* h, int kind, const StageArgs& a) {
   if (!h->prof) return launch_raw(h, kind, a);
   if (2 * (h->ev_used + 1) > h->ev.size()) {
     for (int q = 0; q < 64; ++q) {
@@ -188,10 +266,29 @@ void prof_resolve(gpe_handle* h) {
   h->ev_used = 0;
 }
 
+// Per-axis tables of the solve.  A z-slab takes its rows of the global
+// grid's tables (coordinates, trap, sponge and quadrature weights all belong
+// to the global z axis).
 void build_tables(gpe_handle* h, std::vector<double>& t) {
   std::vector<double>* xyz[3] = {&h->x, &h->y, &h->z};
   double d[3];
-  build_axis_tables(h->p, t, xyz, d);
+  if (!h->slab) {
+    build_axis_tables(h->p, t, xyz, d);
+  } else {
+    gpe_params pg = h->p;
+    pg.nz = h->nz_global;
+    std::vector<double> tg, zg;
+    std::vector<double>* xyzg[3] = {&h->x, &h->y, &zg};
+    build_axis_tables(pg, tg, xyzg, d);
+    const size_t ng = (size_t)pg.nx + pg.ny + pg.nz, nl = (size_t)h->p.nx + h->p.ny + h->p.nz;
+    const size_t nxy = (size_t)pg.nx + pg.ny;
+    t.assign(nl * 4, 0.0);
+    for (int b = 0; b < 4; ++b) {
+      for (size_t q = 0; q < nxy; ++q) t[b * nl + q] = tg[b * ng + q];
+      for (int k = 0; k < h->p.nz; ++k) t[b * nl + nxy + k] = tg[b * ng + nxy + h->k0 + k];
+    }
+    h->z.assign(zg.begin() + h->k0, zg.begin() + h->k0 + h->p.nz);
+  }
   h->dx = d[0];
   h->dy = d[1];
   h->dz = d[2];
@@ -199,7 +296,9 @@ void build_tables(gpe_handle* h, std::vector<double>& t) {
 
 StageArgs base_args(gpe_handle* h) {
   const double d[3] = {h->dx, h->dy, h->dz};
-  return make_base_args(h->p, h->g, h->R, h->zc, d, h->tables);
+  StageArgs a = make_base_args(h->p, h->g, h->R, h->zc, d, h->tables);
+  a.zghost = h->zghost;
+  return a;
 }
 
 int finalize_into(gpe_handle* h, const double* part, int slot) {
@@ -221,9 +320,26 @@ int check_status(gpe_handle* h) {
 }
 
 int fetch_results(gpe_handle* h) {
+  // z-slabs: norms and energies are sums over the slabs, errmax a maximum
+  // (the MPI_ALLREDUCE of src/variables.f90:554-604, src/solve.f90:189-190)
+  if (h->nccl && nccl_reduce_results(h->nccl, h->dres, h->st, h->xerr) != 0)
+    return fail(h, GPE_ERR_CUDA, "z-slab reduction failed");
   CU(h, cudaMemcpyAsync(h->hres, h->dres, 6 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   if (h->prof) prof_resolve(h);
+  if (h->hub && h->hub->n > 1) {
+    SlabHub* hub = h->hub;
+    for (int q = 0; q < 6; ++q) hub->vals[h->rank][q] = h->hres[q];
+    if (!hub->barrier(hub->timeout_s))
+      return fail(h, GPE_ERR_TIMEOUT, "a z-slab of the hub stopped calling in (barrier timeout)");
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int r = 0; r < hub->n; ++r)
+      for (int q = 0; q < 6; ++q)
+        v[q] = (q == 2 || q == 5) ? std::max(v[q], hub->vals[r][q]) : v[q] + hub->vals[r][q];
+    if (!hub->barrier(hub->timeout_s))
+      return fail(h, GPE_ERR_TIMEOUT, "a z-slab of the hub stopped calling in (barrier timeout)");
+    for (int q = 0; q < 6; ++q) h->hres[q] = v[q];
+  }
   return check_status(h);
 }
 
@@ -415,14 +531,16 @@ int ensure_staging(gpe_handle* h, size_t bytes) {
 int pack_from_device(gpe_handle* h, const void* src, int dtype) {
   const int nb = 148 * 8;
   void* dst = h->fields[h->cur];
+  const int zm = h->zghost;
   if (h->esz == 16) {
-    if (dtype == GPE_C128) k_pack<double2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (double2*)dst, h->g, h->R, h->p.bcs);
-    else k_pack<double2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (double2*)dst, h->g, h->R, h->p.bcs);
+    if (dtype == GPE_C128) k_pack<double2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (double2*)dst, h->g, h->R, h->p.bcs, zm);
+    else k_pack<double2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (double2*)dst, h->g, h->R, h->p.bcs, zm);
   } else {
-    if (dtype == GPE_C128) k_pack<float2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (float2*)dst, h->g, h->R, h->p.bcs);
-    else k_pack<float2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (float2*)dst, h->g, h->R, h->p.bcs);
+    if (dtype == GPE_C128) k_pack<float2, double2><<<nb, 256, 0, h->st>>>((const double2*)src, (float2*)dst, h->g, h->R, h->p.bcs, zm);
+    else k_pack<float2, float2><<<nb, 256, 0, h->st>>>((const float2*)src, (float2*)dst, h->g, h->R, h->p.bcs, zm);
   }
   CU(h, cudaGetLastError());
+  CU(h, slab_exchange(h, h->cur));
   return GPE_OK;
 }
 
@@ -464,36 +582,89 @@ int64_t gpe_state_bytes(const gpe_params* p) {
   return (int64_t)padded_elems(g) * esz * nfields(p->scheme);
 }
 
-int gpe_create(const gpe_params* p, gpe_handle** out) {
+}  // extern "C"
+
+namespace {
+
+// which z-slab of a decomposed solve a handle is (null: the whole grid)
+struct SlabSpec {
+  int rank, nranks;
+  const void* nccl_id;
+  SlabHub* hub;
+};
+
+int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
   if (!out) return fail(nullptr, GPE_ERR_BADARG, "null output handle pointer");
   *out = nullptr;
   std::string why;
   if (int rc = validate(p, why)) return fail(nullptr, rc, why);
+  int k0 = 0, nzl = p->nz;
+  if (sp) {
+    if (sp->nranks < 1 || sp->rank < 0 || sp->rank >= sp->nranks)
+      return fail(nullptr, GPE_ERR_BADARG, "gpe_create_slab: rank must be in [0, nranks)");
+    if ((sp->nccl_id != nullptr) == (sp->hub != nullptr))
+      return fail(nullptr, GPE_ERR_BADARG, "gpe_create_slab: give exactly one of nccl_id and hub");
+    if (sp->hub && sp->hub->n != sp->nranks)
+      return fail(nullptr, GPE_ERR_BADARG, "gpe_create_slab: the hub was created for another number of slabs");
+    slab_partition(p->nz, sp->nranks, sp->rank, &k0, &nzl);
+    if (nzl < 6) return fail(nullptr, GPE_ERR_BADARG, "gpe_create_slab: every z-slab needs at least 6 planes");
+    if (sp->hub) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      if (dev != sp->hub->dev)
+        return fail(nullptr, GPE_ERR_BADARG, "gpe_create_slab: the hub's slabs share its device and stream");
+    }
+  }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0)
     return fail(nullptr, GPE_ERR_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
   gpe_handle* h = new gpe_handle();
   h->p = *p;
+  h->nz_global = p->nz;
+  if (sp) {
+    // local geometry of the slab; neighbours and the z faces whose ghosts
+    // the kernels write: a periodic axis is a ring of slabs (one slab
+    // exchanges with itself), a reflective axis mirrors at its two ends
+    h->slab = true;
+    h->rank = sp->rank;
+    h->nranks = sp->nranks;
+    h->k0 = k0;
+    h->p.nz = nzl;
+    if (p->bcs == 1) {
+      h->slab_down = (sp->rank + sp->nranks - 1) % sp->nranks;
+      h->slab_up = (sp->rank + 1) % sp->nranks;
+      h->zghost = 0;
+    } else {
+      h->slab_down = sp->rank > 0 ? sp->rank - 1 : -1;
+      h->slab_up = sp->rank < sp->nranks - 1 ? sp->rank + 1 : -1;
+      h->zghost = (sp->rank == 0 ? 1 : 0) | (sp->rank == sp->nranks - 1 ? 2 : 0);
+    }
+  }
+  const gpe_params& pl = h->p;
   cudaGetDevice(&h->dev);
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, h->dev) != cudaSuccess || prop.major < 10) {
     delete h;
     return fail(nullptr, GPE_ERR_CUDA, "an sm_100 (Blackwell) device is required");
   }
-  layout(p, h->g, h->esz);
+  layout(&pl, h->g, h->esz);
   h->R = p->order / 2;
   h->cmode = p->storage == GPE_C128 ? CM_F64 : (p->compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32);
   h->nelem = padded_elems(h->g);
-  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, p->nz) : choose_zc(h->g);
-  h->grid = dim3((p->nx + 31) / 32, (p->ny + 7) / 8, (p->nz + h->zc - 1) / h->zc);
+  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g);
+  h->grid = dim3((pl.nx + 31) / 32, (pl.ny + 7) / 8, (pl.nz + h->zc - 1) / h->zc);
   h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
   auto bail = [&](int rc) {
     std::string m = h->err;
     gpe_destroy(h);
     return fail(nullptr, rc, m);
   };
-  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+  if (sp && sp->hub) {
+    h->hub = sp->hub;
+    h->st = sp->hub->st;
+    h->own_stream = false;
+  } else if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
     h->err = "cudaStreamCreate failed";
     return bail(GPE_ERR_CUDA);
   }
@@ -541,13 +712,84 @@ int gpe_create(const gpe_params* p, gpe_handle** out) {
     h->err = "initialisation failed";
     return bail(GPE_ERR_CUDA);
   }
+  if (sp && sp->nccl_id && nccl_comm_init(&h->nccl, sp->nranks, sp->nccl_id, sp->rank, h->err) != 0)
+    return bail(GPE_ERR_CUDA);
+  if (sp && sp->hub) {
+    std::lock_guard<std::mutex> lk(sp->hub->mu);
+    sp->hub->slabs[sp->rank] = h;
+  }
   *out = h;
   return GPE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpe_create(const gpe_params* p, gpe_handle** out) { return create_impl(p, nullptr, out); }
+
+int gpe_create_slab(const gpe_params* p, int32_t rank, int32_t nranks, const void* nccl_id, gpe_slab_hub* hub,
+                    gpe_handle** out) {
+  const SlabSpec sp{rank, nranks, nccl_id, hub ? &hub->hub : nullptr};
+  return create_impl(p, &sp, out);
+}
+
+int gpe_slab_partition(int32_t nz, int32_t nranks, int32_t rank, int32_t* k0, int32_t* nzl) {
+  if (nz < 1 || nranks < 1 || rank < 0 || rank >= nranks || !k0 || !nzl) return GPE_ERR_BADARG;
+  int a = 0, b = 0;
+  slab_partition(nz, nranks, rank, &a, &b);
+  *k0 = a;
+  *nzl = b;
+  return GPE_OK;
+}
+
+int gpe_slab_extent(const gpe_handle* h, int32_t* k0, int32_t* nzl) {
+  if (!h || !k0 || !nzl) return GPE_ERR_BADARG;
+  *k0 = h->k0;
+  *nzl = h->p.nz;
+  return GPE_OK;
+}
+
+int gpe_slab_nccl_id(void* id128) {
+  if (!id128) return fail(nullptr, GPE_ERR_BADARG, "null id buffer");
+  std::string why;
+  if (nccl_unique_id(id128, why) != 0) return fail(nullptr, GPE_ERR_CUDA, why);
+  return GPE_OK;
+}
+
+int gpe_slab_hub_create(int32_t nranks, gpe_slab_hub** out) {
+  if (!out || nranks < 1) return fail(nullptr, GPE_ERR_BADARG, "gpe_slab_hub_create: bad arguments");
+  gpe_slab_hub* hb = new gpe_slab_hub();
+  hb->hub.n = nranks;
+  cudaGetDevice(&hb->hub.dev);
+  hb->hub.slabs.assign(nranks, nullptr);
+  hb->hub.vals.assign(nranks, std::array<double, 6>{});
+  // seconds a slab waits at a hub barrier for the others (a slab that stops
+  // calling in breaks the hub and every slab's next call returns
+  // GPE_ERR_TIMEOUT)
+  if (const char* e = getenv("GPE_HUB_TIMEOUT_S")) hb->hub.timeout_s = atof(e) > 0 ? atof(e) : 120.0;
+  if (cudaStreamCreateWithFlags(&hb->hub.st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete hb;
+    return fail(nullptr, GPE_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  *out = hb;
+  return GPE_OK;
+}
+
+void gpe_slab_hub_destroy(gpe_slab_hub* hb) {
+  if (!hb) return;
+  cudaSetDevice(hb->hub.dev);
+  cudaStreamSynchronize(hb->hub.st);
+  cudaStreamDestroy(hb->hub.st);
+  delete hb;
 }
 
 void gpe_destroy(gpe_handle* h) {
   if (!h) return;
   cudaSetDevice(h->dev);
+  // the slabs of a hub read each other's fields: every slab must be done
+  // enqueueing exchanges before any of them frees its memory (collective)
+  if (h->hub && h->hub->slabs[h->rank] == h) h->hub->barrier(h->hub->timeout_s);
   if (h->st) cudaStreamSynchronize(h->st);
   for (void* f : h->fields)
     if (f) cudaFree(f);
@@ -560,7 +802,12 @@ void gpe_destroy(gpe_handle* h) {
   if (h->status) cudaFree(h->status);
   if (h->fft_work) cudaFree(h->fft_work);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
-  if (h->st) cudaStreamDestroy(h->st);
+  if (h->st && h->own_stream) cudaStreamDestroy(h->st);
+  if (h->nccl) nccl_comm_destroy(h->nccl);
+  if (h->hub) {
+    std::lock_guard<std::mutex> lk(h->hub->mu);
+    if (h->hub->slabs[h->rank] == h) h->hub->slabs[h->rank] = nullptr;
+  }
   delete h;
 }
 
@@ -719,6 +966,7 @@ static int ensure_fft(gpe_handle* h) {
 
 int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t* nharm, double* F, int32_t nF) {
   if (!h || !info) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (h->slab) return fail(h, GPE_ERR_BADARG, "gpe_condensed: not available on a z-slab handle");
   if (F && nF != h->p.nx / 2) return fail(h, GPE_ERR_BADARG, "gpe_condensed: nF must be nx/2");
   CU(h, cudaSetDevice(h->dev));
   if (int rc = ensure_fft(h)) return rc;
@@ -758,6 +1006,7 @@ int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t*
 
 int gpe_filtered(gpe_handle* h, double m, double filter_kc, void* out, int32_t dtype) {
   if (!h || !out) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (h->slab) return fail(h, GPE_ERR_BADARG, "gpe_filtered: not available on a z-slab handle");
   if (!(filter_kc > 0.0)) return fail(h, GPE_ERR_BADARG, "gpe_filtered: filter_kc must be > 0");
   if (dtype != GPE_C128 && dtype != GPE_C64) return fail(h, GPE_ERR_BADARG, "gpe_filtered: bad dtype");
   CU(h, cudaSetDevice(h->dev));
@@ -790,6 +1039,7 @@ int gpe_renormalise(gpe_handle* h, double norm) {
 
 int gpe_set_ic(gpe_handle* h, const gpe_ic* ic) {
   if (!h) return GPE_ERR_BADARG;
+  if (h->slab) return fail(h, GPE_ERR_BADARG, "gpe_set_ic: not available on a z-slab handle (use gpe_set_state)");
   std::string why;
   if (int rc = ic_validate(ic, why)) return fail(h, rc, why);
   CU(h, cudaSetDevice(h->dev));

@@ -187,6 +187,7 @@ StageArgs make_base_args(const gpe_params& p, const Geom& g, int R, int zc, cons
     a.izz = 1.0 / (12.0 * dz2);
     a.ix1 = 1.0 / (12.0 * d[0]);
   }
+  a.zghost = 3;
   a.g_nl = p.g;
   a.mu = p.mu;
   a.gamma = p.eqn == 4 ? p.gamma : 0.0;

@@ -80,6 +80,7 @@ struct alignas(16) StageArgs {
   const double *cx, *cy, *cz;   // coordinates (sphere)
   double* partials;             // [nblocks][RED_SLOTS]
   int* status;                  // device status word: non-zero = a bounded wait expired
+  int zghost;                   // z ghosts the producer writes: bit 0 below the grid, bit 1 above
 };
 
 static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is copied in 16-byte words");
@@ -146,6 +147,16 @@ __host__ __device__ __forceinline__ int ghost_pos(int q, int n, int R, int bcs) 
     if (q >= n - 1 - R && q <= n - 2) return 2 * (n - 1) - q;
   }
   return NOGHOST;
+}
+
+// ghost_pos for the z axis of a grid that may be one z-slab of a larger
+// one: ghosts that land below the slab (q < 0) are written only with bit 0
+// of zmask, those above (q >= n) only with bit 1.  A whole grid uses 3; a
+// slab whose face borders another slab leaves that face to the halo exchange.
+__host__ __device__ __forceinline__ int zghost_pos(int k, int n, int R, int bcs, int zmask) {
+  const int q = ghost_pos(k, n, R, bcs);
+  if (q == NOGHOST) return q;
+  return (q < 0 ? (zmask & 1) : (zmask & 2)) ? q : NOGHOST;
 }
 
 // 2nd derivative along one axis, expression order of derivs.f90:164-181
@@ -692,7 +703,7 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
       } else {
         n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
       }
-      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, (long long)(k + 2) * g.pz + col, ghost_pos(k, g.nz, R, a.bcs),
+      site_stage<S, C, R, KIND>(a, n, pv, i, j, k, (long long)(k + 2) * g.pz + col, zghost_pos(k, g.nz, R, a.bcs, a.zghost),
                                 cc, r_norm, r_en, r_err);
     }
 

@@ -285,7 +285,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
 
     if (okw) {
       const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
-      const int gz = (k <= R || k >= g.nz - 1 - R) ? ghost_pos(k, g.nz, R, a.bcs) : NOGHOST;
+      const int gz = (k <= R || k >= g.nz - 1 - R) ? zghost_pos(k, g.nz, R, a.bcs, a.zghost) : NOGHOST;
       Nb<C> n[PY];
       S pv[PY][NPW > 0 ? NPW : 1];
 #pragma unroll

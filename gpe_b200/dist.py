@@ -1,13 +1,15 @@
 """Multi-process plumbing: one process per GPU, torch.distributed for the
 control plane only.
 
-The time-stepper's multi-GPU mode is replicas: independent solves are
-sharded over ranks and advance with no data-path collective.  What crosses
-ranks is bookkeeping: a barrier around timed regions, the max of the ranks'
-device times, sums of throughput counters, and which rank owns which solve.
-(The reference's only decomposition is the (y,z) pencil split of one solve
-with MPI halo exchange, src/variables.f90:186-375; a single solve here fits
-one GPU.)
+Two multi-GPU modes:
+  * replicas (the benchmark's mode): independent solves are sharded over
+    ranks and advance with no data-path collective.  What crosses ranks is
+    bookkeeping: a barrier around timed regions, the max of the ranks'
+    device times, sums of throughput counters, which rank owns which solve.
+  * z-slabs of one solve (slab_solver): the reference's domain
+    decomposition (src/variables.f90:186-375) along z; the halo exchange and
+    the reductions run inside the library over NCCL, and torch.distributed
+    only carries the 128-byte NCCL id from rank 0 to the others.
 """
 from __future__ import annotations
 
@@ -87,3 +89,29 @@ def finalize() -> None:
     if dist.is_available() and dist.is_initialized():
         dist.barrier()
         dist.destroy_process_group()
+
+
+def slab_plan(nz: int):
+    """(rank, nranks, nccl_id, k0, nzl) of this process for a z-slab solve of
+    nz planes: rank 0 creates the NCCL id and broadcasts it; every rank
+    derives its slab from the same partition rule as the library."""
+    from . import slab
+
+    w = world()
+    nid = slab.nccl_unique_id() if w.rank == 0 else None
+    if w.size > 1:
+        import torch.distributed as dist
+
+        box = [nid]
+        dist.broadcast_object_list(box, src=0)
+        nid = box[0]
+    k0, nzl = slab.partition(nz, w.size, w.rank)
+    return w.rank, w.size, nid, k0, nzl
+
+
+def slab_solver(params):
+    """This rank's z-slab of one solve (gpe_create_slab over NCCL)."""
+    from .solver import Solver
+
+    rank, size, nid, _, _ = slab_plan(params.nz)
+    return Solver(params, rank=rank, nranks=size, nccl_id=nid)

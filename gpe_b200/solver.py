@@ -87,14 +87,26 @@ def _check(lib, h, rc: int) -> None:
 class Solver:
     """One device-resident solve."""
 
-    def __init__(self, params: RunParams):
+    def __init__(self, params: RunParams, rank: int | None = None, nranks: int = 1, nccl_id: bytes | None = None,
+                 hub=None):
+        """The whole grid, or with rank/nranks z-slab `rank` of a decomposed
+        solve over NCCL (nccl_id from gpe_b200.slab.nccl_unique_id) or an
+        in-process gpe_b200.slab.SlabHub."""
         self.lib = L.load()
         self.params = params
         self._cp = params.to_c()
         h = C.c_void_p()
-        rc = self.lib.gpe_create(C.byref(self._cp), C.byref(h))
+        if rank is None:
+            rc = self.lib.gpe_create(C.byref(self._cp), C.byref(h))
+        else:
+            idb = C.create_string_buffer(bytes(nccl_id), 128) if nccl_id is not None else None
+            rc = self.lib.gpe_create_slab(C.byref(self._cp), int(rank), int(nranks), idb,
+                                          hub.h if hub is not None else None, C.byref(h))
         _check(self.lib, None, rc)
         self.h = h
+        k0, nzl = C.c_int32(), C.c_int32()
+        self.lib.gpe_slab_extent(self.h, C.byref(k0), C.byref(nzl))
+        self.k0, self.nzl = k0.value, nzl.value
         # src/gpe.f90:78-82
         self.t = 0.0
         self.im_t = 0.0
@@ -123,7 +135,8 @@ class Solver:
     # -- state --------------------------------------------------------------
     @property
     def shape(self) -> tuple[int, int, int]:
-        return (self.params.nz, self.params.ny, self.params.nx)
+        """(nz, ny, nx) of the state this handle holds (its own slab's nz)."""
+        return (self.nzl, self.params.ny, self.params.nx)
 
     def set_state(self, psi: np.ndarray) -> None:
         psi = np.asarray(psi)

@@ -221,6 +221,38 @@ int gpe_condensed(gpe_handle* h, gpe_condensed_info* info, double* eta, int32_t*
  * post-processing (src/io.f90:540-544). */
 int gpe_filtered(gpe_handle* h, double m, double filter_kc, void* out, int32_t dtype);
 
+/* ---------------------------------------------------------------------------
+ * z-slab decomposition of one solve over several GPUs (the reference's MPI
+ * domain decomposition, src/variables.f90:203-375 + src/mpi.f90, with the z
+ * split only).  Slab r of n owns global planes [k0, k0 + nzl) (the first
+ * nz % n slabs get one plane more; every slab needs >= 6).  p describes the
+ * GLOBAL grid.  After every stage the R boundary planes of the stage output
+ * go to the neighbour slabs' ghost planes; norms, energies and the RKF45
+ * error norm are reduced over the slabs, so every slab takes the same step
+ * control decisions.  gpe_set_state / gpe_get_state / gpe_get_site work on
+ * the handle's own slab (nx * ny * nzl, local k); every slab of a solve must
+ * make the same calls in the same order (set_state, step, norm, energy).
+ *
+ * Transports (exactly one of nccl_id / hub):
+ *   nccl_id: one process (rank) per GPU.  Rank 0 calls gpe_slab_nccl_id and
+ *            sends the 128 bytes to the others (MPI_Bcast, a file, a
+ *            torch.distributed store); the exchange is ncclSend/ncclRecv on
+ *            the handle's stream.  NCCL is loaded at run time.
+ *   hub:     the n slabs live in one process on one device, each handle
+ *            driven by its own host thread; they share the hub's stream.
+ *            gpe_destroy of a hub slab is collective too (all slabs of the
+ *            hub call it), and the hub outlives its slabs.
+ * gpe_set_ic and the FFT diagnostics are not available on slab handles. */
+typedef struct gpe_slab_hub gpe_slab_hub;
+
+int gpe_slab_nccl_id(void* id128);
+int gpe_slab_hub_create(int32_t nslabs, gpe_slab_hub** out);
+void gpe_slab_hub_destroy(gpe_slab_hub* hub);
+int gpe_create_slab(const gpe_params* p, int32_t rank, int32_t nranks, const void* nccl_id, gpe_slab_hub* hub,
+                    gpe_handle** out);
+int gpe_slab_extent(const gpe_handle* h, int32_t* k0, int32_t* nzl);
+int gpe_slab_partition(int32_t nz, int32_t nranks, int32_t rank, int32_t* k0, int32_t* nzl);
+
 /* One site of the current state, (re, im) in FP64: the probe of save_time
  * (src/io.f90:136-184, psi at (nx/2, ny/2, nz/2) into psi_time.dat). */
 int gpe_get_site(gpe_handle* h, int32_t i, int32_t j, int32_t k, double* re_im);
