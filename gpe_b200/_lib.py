@@ -120,6 +120,8 @@ _PROTOS = {
                                 C.c_int32]),
     "gpe_filtered": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_int32]),
     "gpe_get_site": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "gpe_snapshot_begin": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gpe_snapshot_wait": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
     "gpe_slab_nccl_id": (C.c_int, [C.c_void_p]),
     "gpe_slab_hub_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "gpe_slab_hub_destroy": (None, [C.c_void_p]),

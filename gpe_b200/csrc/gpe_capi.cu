@@ -100,6 +100,14 @@ struct gpe_handle {
   gpe::SlabHub* hub = nullptr;
   bool own_stream = true;
   std::string xerr;        // detail of a failed exchange, appended to the next error
+  // asynchronous snapshots (gpe_snapshot_begin/wait): a device copy of the
+  // interior streamed to pinned host memory on its own stream
+  void* snap_dev = nullptr;
+  void* snap_host = nullptr;
+  size_t snap_cap = 0, snap_bytes = 0;
+  cudaStream_t snap_st = nullptr;
+  cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+  bool snap_pending = false;
 };
 
 struct gpe_slab_hub {
@@ -802,6 +810,14 @@ void gpe_destroy(gpe_handle* h) {
   if (h->status) cudaFree(h->status);
   if (h->fft_work) cudaFree(h->fft_work);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  if (h->snap_st) {
+    cudaStreamSynchronize(h->snap_st);
+    cudaStreamDestroy(h->snap_st);
+  }
+  if (h->snap_ready) cudaEventDestroy(h->snap_ready);
+  if (h->snap_done) cudaEventDestroy(h->snap_done);
+  if (h->snap_dev) cudaFree(h->snap_dev);
+  if (h->snap_host) cudaFreeHost(h->snap_host);
   if (h->st && h->own_stream) cudaStreamDestroy(h->st);
   if (h->nccl) nccl_comm_destroy(h->nccl);
   if (h->hub) {
@@ -1061,6 +1077,50 @@ int gpe_get_grid(const gpe_handle* h, double* x, double* y, double* z, double* d
     dxyz[1] = h->dy;
     dxyz[2] = h->dz;
   }
+  return GPE_OK;
+}
+
+int gpe_snapshot_begin(gpe_handle* h, int32_t dtype) {
+  if (!h) return GPE_ERR_BADARG;
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  const size_t bytes = interior_bytes(h, dtype);
+  if (!h->snap_st) {
+    CU(h, cudaStreamCreateWithFlags(&h->snap_st, cudaStreamNonBlocking));
+    CU(h, cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+    CU(h, cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+  }
+  if (h->snap_cap < bytes) {
+    // the previous snapshot's copy must be done with the old buffers
+    CU(h, cudaStreamSynchronize(h->snap_st));
+    if (h->snap_dev) cudaFree(h->snap_dev);
+    if (h->snap_host) cudaFreeHost(h->snap_host);
+    h->snap_dev = h->snap_host = nullptr;
+    h->snap_cap = 0;
+    CU(h, cudaMalloc(&h->snap_dev, bytes));
+    CU(h, cudaMallocHost(&h->snap_host, bytes));
+    h->snap_cap = bytes;
+  } else if (h->snap_pending) {
+    // the device copy of the new snapshot must not overwrite the buffer the
+    // previous transfer still reads (device-side order, the host does not wait)
+    CU(h, cudaStreamWaitEvent(h->st, h->snap_done, 0));
+  }
+  if (int rc = unpack_to_device(h, h->snap_dev, dtype)) return rc;
+  CU(h, cudaEventRecord(h->snap_ready, h->st));
+  CU(h, cudaStreamWaitEvent(h->snap_st, h->snap_ready, 0));
+  CU(h, cudaMemcpyAsync(h->snap_host, h->snap_dev, bytes, cudaMemcpyDeviceToHost, h->snap_st));
+  CU(h, cudaEventRecord(h->snap_done, h->snap_st));
+  h->snap_bytes = bytes;
+  h->snap_pending = true;
+  return GPE_OK;
+}
+
+int gpe_snapshot_wait(gpe_handle* h, const void** host_data, size_t* bytes) {
+  if (!h || !host_data || !bytes) return GPE_ERR_BADARG;
+  if (!h->snap_pending) return GPE_ERR_STATE;
+  if (cudaEventSynchronize(h->snap_done) != cudaSuccess) return GPE_ERR_CUDA;
+  *host_data = h->snap_host;
+  *bytes = h->snap_bytes;
   return GPE_OK;
 }
 

@@ -34,6 +34,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../../include/gpe_cuda.h"
@@ -405,6 +406,14 @@ struct Ctx {
   std::complex<double> dt;
   int64_t p = 0;
   std::vector<double> x, y, z;
+  std::thread writer;  // background writer of the last snapshot (one at a time)
+};
+
+// The run's metadata at the moment a snapshot was taken.
+struct Meta {
+  int64_t p;
+  double t, im_t;
+  std::complex<double> dt;
 };
 
 void check(Ctx& c, int rc) {
@@ -428,29 +437,59 @@ void wr_real(FILE* f, const Ctx& c, double v) {
 }
 
 // end_state (src/io.f90:831-882): stream file proc0000/end_state.dat
-void end_state(Ctx& c, bool final_) {
+void write_end_state(const Ctx& c, const Meta& m, const void* data, size_t bytes) {
   mkdir(path("proc0000").c_str(), 0755);
   FILE* f = fopen(path("proc0000/end_state.dat").c_str(), "wb");
   if (!f) emergency_stop("ERROR: cannot write proc0000/end_state.dat");
   wr_int(f, c.P.nx);
   wr_int(f, c.P.ny);
   wr_int(f, c.P.nz);
-  wr_int(f, (int32_t)c.p);
-  wr_real(f, c, c.t);
-  wr_real(f, c, c.im_t);
-  wr_real(f, c, c.dt.real());
-  wr_real(f, c, c.dt.imag());
-  const auto b = state_bytes(c);
-  fwrite(b.data(), 1, b.size(), f);
+  wr_int(f, (int32_t)m.p);
+  wr_real(f, c, m.t);
+  wr_real(f, c, m.im_t);
+  wr_real(f, c, m.dt.real());
+  wr_real(f, c, m.dt.imag());
+  fwrite(data, 1, bytes, f);
   fclose(f);
   FILE* s = fopen(path("save.dat").c_str(), "w");
   if (s) {
-    fprintf(s, " Periodically saved state\n t = %25.16E\n im_t = %25.16E\n dt = (%25.16E,%25.16E)\n", c.t, c.im_t,
-            c.dt.real(), c.dt.imag());
-    fprintf(s, " nx = %12d\n ny = %12d\n nz = %12d\n p = %12lld\n", c.P.nx, c.P.ny, c.P.nz, (long long)c.p);
+    fprintf(s, " Periodically saved state\n t = %25.16E\n im_t = %25.16E\n dt = (%25.16E,%25.16E)\n", m.t, m.im_t,
+            m.dt.real(), m.dt.imag());
+    fprintf(s, " nx = %12d\n ny = %12d\n nz = %12d\n p = %12lld\n", c.P.nx, c.P.ny, c.P.nz, (long long)m.p);
     fclose(s);
   }
-  if (final_) unlink(path("RUNNING").c_str());
+}
+
+Meta meta(const Ctx& c) { return Meta{c.p, c.t, c.im_t, c.dt}; }
+
+void join_writer(Ctx& c) {
+  if (c.writer.joinable()) c.writer.join();
+}
+
+// Take a snapshot of the state now and hand it to a writer thread; the time
+// loop continues while the device-to-host copy and the file write run.
+template <class Write>
+void write_async(Ctx& c, Write w) {
+  join_writer(c);  // the snapshot buffer is reused
+  check(c, gpe_snapshot_begin(c.h, c.esz == 16 ? GPE_C128 : GPE_C64));
+  const Meta m = meta(c);
+  c.writer = std::thread([&c, m, w]() {
+    const void* data = nullptr;
+    size_t bytes = 0;
+    if (gpe_snapshot_wait(c.h, &data, &bytes) != GPE_OK) emergency_stop("ERROR: snapshot copy failed");
+    w(m, data, bytes);
+  });
+}
+
+void end_state(Ctx& c, bool final_) {
+  if (!final_) {
+    write_async(c, [&c](const Meta& m, const void* d, size_t n) { write_end_state(c, m, d, n); });
+    return;
+  }
+  join_writer(c);
+  const auto b = state_bytes(c);
+  write_end_state(c, meta(c), b.data(), b.size());
+  unlink(path("RUNNING").c_str());
 }
 
 // state_restart (src/ic.f90:117-191) from end_state0000.dat
@@ -500,23 +539,27 @@ std::string itos(int64_t n) {
   return d;
 }
 
-// idl_surface (src/io.f90:480-520): proc0000/dens<itos(p)>.dat + p_saved.dat
-void idl_surface(Ctx& c) {
+// idl_surface (src/io.f90:480-520): proc0000/dens<itos(p)>.dat + p_saved.dat,
+// written from a snapshot on the writer thread
+void write_dens(const Ctx& c, const Meta& m, const void* data, size_t bytes) {
   mkdir(path("proc0000").c_str(), 0755);
-  const std::string name = "proc0000/dens" + itos(c.p) + ".dat";
+  const std::string name = "proc0000/dens" + itos(m.p) + ".dat";
   FILE* f = fopen(path(name).c_str(), "wb");
   if (!f) emergency_stop("ERROR: cannot write " + name);
-  wr_real(f, c, c.t + c.im_t);
+  wr_real(f, c, m.t + m.im_t);
   for (int v : {c.P.nx, c.P.ny, c.P.nz, 1, 1, 0, c.P.ny - 1, 0, c.P.nz - 1}) wr_int(f, v);
-  const auto b = state_bytes(c);
-  fwrite(b.data(), 1, b.size(), f);
+  fwrite(data, 1, bytes, f);
   for (double v : c.x) wr_real(f, c, v);
   for (double v : c.y) wr_real(f, c, v);
   for (double v : c.z) wr_real(f, c, v);
   fclose(f);
   char rec[32];
-  snprintf(rec, sizeof rec, "%10lld", (long long)c.p);
+  snprintf(rec, sizeof rec, "%10lld", (long long)m.p);
   append_line("p_saved.dat", rec);
+}
+
+void idl_surface(Ctx& c) {
+  write_async(c, [&c](const Meta& m, const void* d, size_t n) { write_dens(c, m, d, n); });
 }
 
 double fmodulo(double a, double b) { return a - std::floor(a / b) * b; }
@@ -730,6 +773,7 @@ int main(int argc, char** argv) {
   }
   end_state(c, true);
   if (c.r.save_3d) idl_surface(c);
+  join_writer(c);
   gpe_destroy(c.h);
   printf(" DONE!\n");
   return 0;

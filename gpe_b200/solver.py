@@ -155,6 +155,19 @@ class Solver:
         _check(self.lib, self.h, self.lib.gpe_get_state(self.h, out.ctypes.data, code))
         return out
 
+    def snapshot_begin(self, dtype=np.complex128) -> None:
+        """Start an asynchronous copy of the current state to host memory."""
+        code = L.GPE_C64 if np.dtype(dtype) == np.complex64 else L.GPE_C128
+        _check(self.lib, self.h, self.lib.gpe_snapshot_begin(self.h, code))
+        self._snap_dtype = np.dtype(dtype)
+
+    def snapshot_wait(self) -> np.ndarray:
+        """The state captured by the last snapshot_begin (a copy)."""
+        ptr, n = C.c_void_p(), C.c_size_t()
+        _check(self.lib, self.h, self.lib.gpe_snapshot_wait(self.h, C.byref(ptr), C.byref(n)))
+        buf = (C.c_char * n.value).from_address(ptr.value)
+        return np.frombuffer(buf, dtype=self._snap_dtype).reshape(self.shape).copy()
+
     def set_ic(self, spec) -> None:
         """Generate the initial state on the device (see ic.device_spec)."""
         _check(self.lib, self.h, self.lib.gpe_set_ic(self.h, C.byref(spec)))

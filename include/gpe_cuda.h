@@ -253,6 +253,20 @@ int gpe_create_slab(const gpe_params* p, int32_t rank, int32_t nranks, const voi
 int gpe_slab_extent(const gpe_handle* h, int32_t* k0, int32_t* nzl);
 int gpe_slab_partition(int32_t nz, int32_t nranks, int32_t rank, int32_t* k0, int32_t* nzl);
 
+/* Asynchronous snapshots for checkpoint writers (end_state, dens, filtered
+ * files: src/io.f90:480-520, 831-882).  gpe_snapshot_begin copies the
+ * current state (interior, dtype) on the device, in stream order, and
+ * streams it to a pinned host buffer owned by the handle on a separate
+ * stream; it returns at once and stepping may continue.  gpe_snapshot_wait
+ * blocks until the copy has landed and returns the buffer (nx*ny*nz
+ * complex, x fastest), valid until the next gpe_snapshot_begin.  It touches
+ * no other handle state, so a writer thread may call it while another
+ * thread steps the handle; gpe_snapshot_begin itself belongs to the
+ * stepping thread.  No reference counterpart: the reference writes from the
+ * live array and stalls the time loop meanwhile. */
+int gpe_snapshot_begin(gpe_handle* h, int32_t dtype);
+int gpe_snapshot_wait(gpe_handle* h, const void** host_data, size_t* bytes);
+
 /* One site of the current state, (re, im) in FP64: the probe of save_time
  * (src/io.f90:136-184, psi at (nx/2, ny/2, nz/2) into psi_time.dat). */
 int gpe_get_site(gpe_handle* h, int32_t i, int32_t j, int32_t k, double* re_im);

@@ -138,3 +138,28 @@ def test_host_diagnostics_outputs(gpu, tmp_path):
     assert v[3] == pytest.approx(c.imag, rel=1e-8, abs=1e-12)
     assert v[4] == pytest.approx(abs(c) ** 2, rel=1e-8, abs=1e-12)
     assert v[5] == pytest.approx(np.arctan2(c.imag + 1e-6, c.real), rel=1e-8, abs=1e-12)
+
+
+def test_host_async_snapshots_hold_the_state_of_their_step(gpu, tmp_path):
+    """dens<p>.dat files are written by a background thread from device
+    snapshots while the time loop continues: each must hold the state of
+    step p exactly."""
+    d = tmp_path / "run"
+    shutil.copytree(INPUTS / "ring64", d)
+    t_in = (d / "run.in").read_text()
+    t_in = t_in.replace("save_rate2    = 100.0", "save_rate2    = 0.03")
+    t_in = t_in.replace("save_3d       = .false.", "save_3d       = .true.")
+    (d / "run.in").write_text(t_in)
+    run(d)
+    saved = [int(x) for x in (d / "p_saved.dat").read_text().split()]
+    assert 3 in saved and 6 in saved and 10 in saved
+    s = Solver(RP)
+    s.set_ic(ic.device_spec("ring", ring=dict(plane="xy", r0=4.0)))
+    done = 0
+    n = RP.nx * RP.ny * RP.nz
+    for p in sorted(set(saved)):
+        s.solver(p - done)
+        done = p
+        b = (d / "proc0000" / f"dens{p:07d}.dat").read_bytes()
+        psi = np.frombuffer(b[8 + 36:8 + 36 + 16 * n], dtype=np.complex128).reshape(RP.nz, RP.ny, RP.nx)
+        np.testing.assert_array_equal(psi, s.get_state())

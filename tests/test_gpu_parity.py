@@ -232,3 +232,23 @@ def test_c2_256_cubed_periodic_o4(gpu):
     o, ref, s, out, info = run_both(rp, psi0, 4, want_norm=True)
     assert rel_l2(out, ref) <= TOL64
     assert info.norm == pytest.approx(o.get_norm(ref), rel=TOL64)
+
+
+def test_snapshot_while_stepping(gpu):
+    """gpe_snapshot_begin captures the state of its point in the stream even
+    when stepping continues before gpe_snapshot_wait."""
+    rp = c1_params(nx=40, ny=36, nz=32, xr=9.75, yr=8.75, zr=7.75)
+    psi0 = ic.vortex_ring(rp, "xy", r0=3.0)
+    s = Solver(rp)
+    s.set_state(psi0)
+    s.solver(5)
+    at5 = s.get_state()
+    s.snapshot_begin()
+    s.solver(7, wait=False)
+    snap = s.snapshot_wait()
+    np.testing.assert_array_equal(snap, at5)
+    s.snapshot_begin(np.complex64)
+    s.sync()
+    at12 = s.get_state()
+    np.testing.assert_array_equal(s.snapshot_wait(), at12.astype(np.complex64))
+    s.close()
