@@ -273,6 +273,7 @@ def rk45_leg(args, torch):
 
 
 C4_STEPS = 500
+C4_SHORT = 200
 
 
 def batched_leg(args, torch):
@@ -283,6 +284,7 @@ def batched_leg(args, torch):
     reductions, tile_zc per size from the autotuner.  Timed on the host clock
     from the first submission to the last retired result (state upload and
     download included); latencies are per solve, all submitted at t = 0."""
+    from gpe_b200 import _lib as L
     from gpe_b200 import autotune
     from gpe_b200 import ic
     from gpe_b200.pool import Pool
@@ -300,29 +302,48 @@ def batched_leg(args, torch):
                        order=order, g=1.0, mu=1.0, storage="c64",
                        tile_zc=autotune.best_zc(n, order, "c64", cache))
         psi = ic.vortex_ring(rp, "xy", r0=r0) if k % 2 == 0 else ic.random_phase(rp, seed=k, kc=kc)
-        solves.append((rp, psi.astype(np.complex64)))
+        # the caller's input and result buffers: page-locked, allocated once
+        host = L.pinned_empty(psi.shape, np.complex64)
+        host[...] = psi
+        solves.append((rp, host, L.pinned_empty(psi.shape, np.complex64)))
     autotune.save_cache(cache)
-    budget = sum(Pool.solve_bytes(rp) for rp, _ in solves) + (256 << 20)
-    warm = Pool(budget)
-    for k, (rp, psi) in enumerate(solves):
-        warm.submit(rp, psi, 2, k)
-    warm.run_all()
-    warm.close()
+    budget = sum(Pool.solve_bytes(rp) for rp, _, _ in solves) + (256 << 20)
+    sites = sum(rp.nx * rp.ny * rp.nz for rp, _, _ in solves)
+
+    def run(steps):
+        pool = Pool(budget)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k, (rp, psi, out) in enumerate(solves):
+            assert pool.submit(rp, psi, steps, k, out=out)
+        res = pool.run_all(max_steps=steps)
+        wall = time.perf_counter() - t0
+        pool.close()
+        return wall, res
+
+    run(2)  # warm-up: autotuned shapes, graph capture paths, first-touch
+    wall, res = run(C4_STEPS)
+    lat = np.array([r.finish_s - r.submit_s for r in res])
+    # the same mix resident on the device: time C4_SHORT steps of all solves
     pool = Pool(budget)
+    for k, (rp, psi, out) in enumerate(solves):
+        assert pool.submit(rp, psi, C4_SHORT + 20, k, out=out)
+    pool.step(10)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for k, (rp, psi) in enumerate(solves):
-        assert pool.submit(rp, psi, C4_STEPS, k)
-    res = pool.run_all(max_steps=C4_STEPS)
-    wall = time.perf_counter() - t0
+    pool.step(C4_SHORT)
+    torch.cuda.synchronize()
+    resident = time.perf_counter() - t0
+    pool.run_all()
     pool.close()
-    sites = sum(rp.nx * rp.ny * rp.nz for rp, _ in solves)
-    lat = np.array([r.finish_s - r.submit_s for r in res])
     return {"value": sites * C4_STEPS / wall, "unit": UNIT, "solves": len(res), "sites": sites,
             "steps": C4_STEPS, "wall_s": wall, "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "storage": "c64",
+            "stepping_rate": sites * C4_SHORT / resident,
             "tile_zc": {k: v["zc"] for k, v in cache.items()},
-            "timing": "host clock, first submit to last result, uploads/downloads included"}
+            "timing": "value: host clock, first submit to last result, uploads/downloads included (the caller's "
+                      "states and result buffers in page-locked host memory); stepping_rate: host clock around "
+                      f"{C4_SHORT} steps of the whole mix resident on the device (synchronised both sides)"}
 
 
 def run_serving(args) -> int:
@@ -488,6 +509,7 @@ def main() -> int:
         line["rk45_trapped"] = rk45_leg(args, torch)
         line["batched_c4"] = batched_leg(args, torch)
         line["batched_c4"]["speedup_vs_plain_fp64"] = line["batched_c4"]["value"] / (value / ws)
+        line["batched_c4"]["stepping_speedup_vs_plain_fp64"] = line["batched_c4"]["stepping_rate"] / (value / ws)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     s.close()

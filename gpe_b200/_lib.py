@@ -122,6 +122,8 @@ _PROTOS = {
     "gpe_get_site": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "gpe_snapshot_begin": (C.c_int, [C.c_void_p, C.c_int32]),
     "gpe_snapshot_wait": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "gpe_host_alloc": (C.c_void_p, [C.c_size_t]),
+    "gpe_host_free": (None, [C.c_void_p]),
     "gpe_slab_nccl_id": (C.c_int, [C.c_void_p]),
     "gpe_slab_hub_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "gpe_slab_hub_destroy": (None, [C.c_void_p]),
@@ -172,3 +174,21 @@ def load() -> C.CDLL:
 
 def declared_symbols() -> list[str]:
     return list(_PROTOS)
+
+
+def pinned_empty(shape, dtype) -> "np.ndarray":
+    """An uninitialised numpy array in page-locked host memory
+    (gpe_host_alloc), freed when the array is garbage-collected."""
+    import weakref
+
+    import numpy as np
+
+    lib = load()
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    ptr = lib.gpe_host_alloc(max(nbytes, 1))
+    if not ptr:
+        raise MemoryError("gpe_host_alloc failed")
+    buf = (C.c_char * max(nbytes, 1)).from_address(ptr)
+    weakref.finalize(buf, lib.gpe_host_free, ptr)
+    return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)

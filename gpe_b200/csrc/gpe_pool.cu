@@ -702,15 +702,19 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
   for (int cm = 0; cm < NCM; ++cm)
     for (int fam = 0; fam < NFAM; ++fam) {
       Class& c = P->cls[cm][fam];
-      std::vector<Solve*> keep;
+      std::vector<Solve*> keep, fin;
       bool retired = false;
       for (Solve* s : c.solves) {
         if (s->done < s->nsteps && s->status == GPE_OK) {
           keep.push_back(s);
           continue;
         }
+        // all finished states go down back to back, one synchronisation
         if (int rc = download_state(P, s, s->fam == FAM_RK45 ? s->cur : 0)) return rc;
-        PCU(P, cudaStreamSynchronize(P->st));
+        fin.push_back(s);
+      }
+      if (!fin.empty()) PCU(P, cudaStreamSynchronize(P->st));
+      for (Solve* s : fin) {
         gpe_result r;
         memset(&r, 0, sizeof(r));
         r.tag = s->tag;
@@ -751,6 +755,19 @@ int gpe_pool_poll(gpe_pool* P, gpe_result* out, int32_t max, int32_t* n_out) {
 }
 
 int64_t gpe_pool_free_bytes(const gpe_pool* P) { return P ? (int64_t)P->alloc.free_bytes() : -1; }
+
+void* gpe_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0 || cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void gpe_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
 
 const char* gpe_pool_last_error(const gpe_pool* P) { return P ? P->err.c_str() : ""; }
 

@@ -383,12 +383,14 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_batch(const BatchStage* 
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   const int tid = threadIdx.y * 32 + threadIdx.x;
+  int fenced = -1;  // solve whose tensor maps thread 0 has acquired (they do not change within a launch)
   for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
     const BatchItem it = items[w];
     const BatchStage* bs = tab + it.solve;
-    if (tid == 0) {
+    if (tid == 0 && it.solve != fenced) {
       tensormap_acquire(&bs->maps.in);
       for (int f = 0; f < StageTraits<KIND>::NPW; ++f) tensormap_acquire(&bs->maps.pw[f]);
+      fenced = it.solve;
     }
     // the item's arguments in registers (read-only path, same address for
     // every thread); a shared-memory copy would be re-read after every

@@ -72,14 +72,20 @@ class Pool:
     def free_bytes(self) -> int:
         return int(self.lib.gpe_pool_free_bytes(self.h))
 
-    def submit(self, params: RunParams, psi0: np.ndarray, nsteps: int, tag: int) -> bool:
-        """Admit a solve; False when it does not fit in the free budget."""
+    def submit(self, params: RunParams, psi0: np.ndarray, nsteps: int, tag: int,
+               out: np.ndarray | None = None) -> bool:
+        """Admit a solve; False when it does not fit in the free budget.  The
+        final state is written to `out` (default: a new array); a reused
+        buffer from gpe_b200._lib.pinned_empty makes the copy back a DMA."""
         dt = np.complex64 if params.storage == "c64" else np.complex128
         code = L.GPE_C64 if params.storage == "c64" else L.GPE_C128
         psi = np.ascontiguousarray(psi0, dtype=dt)
         if psi.shape != (params.nz, params.ny, params.nx):
             raise ValueError("psi0 must have shape (nz, ny, nx)")
-        out = np.empty_like(psi)
+        if out is None:
+            out = np.empty_like(psi)
+        elif out.shape != psi.shape or out.dtype != psi.dtype or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous array of psi0's shape and dtype")
         cp = params.to_c()
         rc = self.lib.gpe_pool_submit(self.h, C.byref(cp), psi.ctypes.data, code, int(nsteps), int(tag),
                                       out.ctypes.data)
@@ -90,10 +96,14 @@ class Pool:
         self._out[int(tag)] = out
         return True
 
-    def submit_ic(self, params: RunParams, spec, nsteps: int, tag: int) -> bool:
+    def submit_ic(self, params: RunParams, spec, nsteps: int, tag: int, out: np.ndarray | None = None) -> bool:
         """Admit a solve whose initial state is generated on the device."""
         dt = np.complex64 if params.storage == "c64" else np.complex128
-        out = np.empty((params.nz, params.ny, params.nx), dtype=dt)
+        shape = (params.nz, params.ny, params.nx)
+        if out is None:
+            out = np.empty(shape, dtype=dt)
+        elif out.shape != shape or out.dtype != np.dtype(dt) or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous (nz, ny, nx) array of the storage dtype")
         cp = params.to_c()
         rc = self.lib.gpe_pool_submit_ic(self.h, C.byref(cp), C.byref(spec), int(nsteps), int(tag),
                                          out.ctypes.data)

@@ -333,6 +333,13 @@ int64_t gpe_pool_free_bytes(const gpe_pool* pool);
 /* Arena bytes one solve with these parameters needs (state + tables). */
 int64_t gpe_pool_solve_bytes(const gpe_params* p);
 const char* gpe_pool_last_error(const gpe_pool* pool);
+
+/* Page-locked host memory (cudaMallocHost) for the psi0 / out buffers of
+ * gpe_pool_submit and the host arrays of gpe_set_state / gpe_get_state:
+ * copies to and from it run at DMA speed and asynchronously, where pageable
+ * memory is staged by the driver.  NULL on failure. */
+void* gpe_host_alloc(size_t bytes);
+void gpe_host_free(void* p);
 void gpe_pool_destroy(gpe_pool* pool);
 
 /* Bytes of device memory a solve with these parameters allocates. */
