@@ -166,6 +166,31 @@ def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime:
     return rep
 
 
+class ResultBuffers:
+    """Page-locked result buffers reused across requests of the same shape:
+    a finished solve's state lands by DMA, and the buffer goes back to the
+    free list once the result has been handed on."""
+
+    def __init__(self):
+        self._free: dict[tuple, list[np.ndarray]] = {}
+
+    def get(self, shape, dtype) -> np.ndarray:
+        key = (tuple(shape), np.dtype(dtype).str)
+        lst = self._free.get(key)
+        if lst:
+            return lst.pop()
+        from . import _lib as L
+
+        return L.pinned_empty(shape, dtype)
+
+    def put(self, arr: np.ndarray) -> None:
+        self._free.setdefault((arr.shape, arr.dtype.str), []).append(arr)
+
+
+def _storage_dtype(params) -> np.dtype:
+    return np.dtype(np.complex64 if params.storage == "c64" else np.complex128)
+
+
 def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites) -> ServeReport:
     """Admission is first-come first-served, bounded by the HBM budget and by
     max_active_sites: enough grid sites in flight to keep the GPU's memory
@@ -173,6 +198,7 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
     later arrival."""
     pool = Pool(budget_bytes)
     rep = ServeReport()
+    bufs = ResultBuffers()
     pending = sorted(requests, key=lambda r: r.arrival_s)
     by_tag = {r.tag: r for r in requests}
     waiting: list[Request] = []
@@ -190,10 +216,13 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
             if active and active_sites + req.sites > max_active_sites:
                 still.extend(waiting[q:])  # first come, first served
                 break
-            if pool.submit_ic(req.params, device_ic(req), req.nsteps, req.tag):
+            p = req.params
+            out = bufs.get((p.nz, p.ny, p.nx), _storage_dtype(p))
+            if pool.submit_ic(p, device_ic(req), req.nsteps, req.tag, out=out):
                 active += 1
                 active_sites += req.sites
             else:
+                bufs.put(out)
                 rep.rejected_admissions += 1
                 still.extend(waiting[q:])
                 break
@@ -209,6 +238,7 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
             rep.latencies_s[r.tag] = done_t - req.arrival_s
             rep.site_updates += req.sites * r.steps
             active_sites -= req.sites
+            bufs.put(r.psi)  # the state has been delivered; the buffer serves the next request
     rep.wall_s = time.perf_counter() - t0
     pool.close()
     return rep
@@ -221,6 +251,7 @@ def serve_one_at_a_time(requests: list[Request], realtime: bool = True) -> Serve
     from .solver import Solver
 
     rep = ServeReport()
+    bufs = ResultBuffers()
     t0 = time.perf_counter()
     for req in sorted(requests, key=lambda r: r.arrival_s):
         if realtime:
@@ -230,6 +261,9 @@ def serve_one_at_a_time(requests: list[Request], realtime: bool = True) -> Serve
         s = Solver(req.params.replace(storage="c128", compute="auto"))
         s.set_ic(device_ic(req))
         s.solver(req.nsteps)
+        out = bufs.get(s.shape, np.complex128)
+        s.get_state(out=out)  # the result is delivered, as in the batched loop
+        bufs.put(out)
         s.close()
         rep.latencies_s[req.tag] = time.perf_counter() - t0 - req.arrival_s
         rep.site_updates += req.sites * req.nsteps
