@@ -108,6 +108,10 @@ struct gpe_handle {
   cudaStream_t snap_st = nullptr;
   cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
   bool snap_pending = false;
+  // one captured RK4/RK2 step without reductions, replayed by gpe_step
+  // (the stage arguments, dt included, are baked into the graph)
+  cudaGraphExec_t step_graph = nullptr;
+  double graph_dr = 0, graph_di = 0;
 };
 
 struct gpe_slab_hub {
@@ -810,6 +814,7 @@ void gpe_destroy(gpe_handle* h) {
   if (h->status) cudaFree(h->status);
   if (h->fft_work) cudaFree(h->fft_work);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
   if (h->snap_st) {
     cudaStreamSynchronize(h->snap_st);
     cudaStreamDestroy(h->snap_st);
@@ -871,6 +876,39 @@ int gpe_get_state_device(gpe_handle* h, void* psi_dev, int32_t dtype) {
   return GPE_OK;
 }
 
+// Graph of one fixed step for the current dt (captured on first use and
+// whenever dt changes).  Only for schemes that keep psi in place.
+static int ensure_step_graph(gpe_handle* h, double dr, double di) {
+  if (h->step_graph && h->graph_dr == dr && h->graph_di == di) return GPE_OK;
+  if (h->step_graph) {
+    cudaGraphExecDestroy(h->step_graph);
+    h->step_graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CU(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue_fixed_step(h, dr, di, false, false);
+  const cudaError_t e = cudaStreamEndCapture(h->st, &g);
+  if (rc != GPE_OK) {
+    if (e == cudaSuccess && g) cudaGraphDestroy(g);
+    return rc;
+  }
+  CU(h, e);
+  const cudaError_t ei = cudaGraphInstantiate(&h->step_graph, g, 0);
+  cudaGraphDestroy(g);
+  CU(h, ei);
+  h->graph_dr = dr;
+  h->graph_di = di;
+  return GPE_OK;
+}
+
+static bool use_step_graphs(const gpe_handle* h) {
+  static const bool off = [] {
+    const char* e = getenv("GPE_GRAPHS");
+    return e && atoi(e) == 0;
+  }();
+  return !off && !h->prof && !h->slab && (h->p.scheme == GPE_RK4 || h->p.scheme == GPE_RK2);
+}
+
 static int step_impl(gpe_handle* h, int64_t nsteps, gpe_step_info* io, bool wait) {
   if (!h || !io || nsteps < 0) return fail(h, GPE_ERR_BADARG, "bad gpe_step arguments");
   CU(h, cudaSetDevice(h->dev));
@@ -887,8 +925,18 @@ static int step_impl(gpe_handle* h, int64_t nsteps, gpe_step_info* io, bool wait
     }
   } else {
     const double dr = io->dt_re, di = io->dt_im;
+    // steps without reductions replay a captured graph (one launch instead of
+    // one per stage); the first step of a call runs plainly, so every kernel
+    // has been loaded and configured before any capture
+    const bool graphs = use_step_graphs(h) && nsteps >= 3;
     for (int64_t s = 0; s < nsteps; ++s) {
-      if (int rc = enqueue_fixed_step(h, dr, di, want_e && s == 0, want_n && s == nsteps - 1)) return rc;
+      const bool e = want_e && s == 0, n = want_n && s == nsteps - 1;
+      if (graphs && s > 0 && !e && !n) {
+        if (int rc = ensure_step_graph(h, dr, di)) return rc;
+        CU(h, cudaGraphLaunch(h->step_graph, h->st));
+      } else if (int rc = enqueue_fixed_step(h, dr, di, e, n)) {
+        return rc;
+      }
       io->t = io->t + dr;
       io->im_t = io->im_t + fabs(di);
       io->p += 1;
