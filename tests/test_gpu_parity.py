@@ -252,3 +252,29 @@ def test_snapshot_while_stepping(gpu):
     at12 = s.get_state()
     np.testing.assert_array_equal(s.snapshot_wait(), at12.astype(np.complex64))
     s.close()
+
+
+@pytest.mark.parametrize("shape", [(6, 6, 6), (7, 6, 9), (33, 6, 7)])
+@pytest.mark.parametrize("order,bcs", [(2, 1), (2, 2), (4, 1), (4, 2)])
+@pytest.mark.parametrize("scheme", ["euler", "rk4", "rk45"])
+def test_smallest_grids_match_oracle(gpu, shape, order, bcs, scheme):
+    """The smallest admitted grids (6 points per axis): every site sits next
+    to a ghost face, tiles are mostly empty, and a z-chunk holds the whole
+    axis; (33, 6, 7) also puts one site in a second x tile."""
+    nx, ny, nz = shape
+    rp = RunParams(nx=nx, ny=ny, nz=nz, xr=0.5 * (nx - 1), yr=0.5 * (ny - 1), zr=0.5 * (nz - 1), tau=0.005,
+                   scheme=scheme, eqn_to_solve=4, bcs=bcs, order=order, g=1.0, mu=2.0, omx=0.3, omy=0.2, omz=0.25)
+    rng = np.random.default_rng(nx * 100 + ny * 10 + nz + order + bcs)
+    psi0 = 1.0 + 0.2 * (rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx)))
+    o, ref, s, out, info = run_both(rp, psi0, 12, want_norm=True)
+    tol = 1e-10 if scheme == "rk45" else TOL64
+    assert rel_l2(out, ref) <= tol
+    assert info.norm == pytest.approx(o.get_norm(ref), rel=tol)
+    s.close()
+
+
+def test_grid_below_the_minimum_is_rejected(gpu):
+    rp = RunParams(nx=5, ny=8, nz=8, xr=2.0, yr=3.5, zr=3.5)
+    with pytest.raises(L.GpeError) as e:
+        Solver(rp)
+    assert e.value.code == L.GPE_ERR_BADARG
