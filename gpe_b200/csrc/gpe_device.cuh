@@ -202,14 +202,20 @@ __device__ __forceinline__ void store_with_ghosts(S* f, const Geom& g, long long
   if (gz != NOGHOST) f[(long long)(gz + 2) * g.pz + col] = v;
 }
 
-// Same with the centre offset o of (i,j,k) already known.
-template <class S>
+// Same with the centre offset o of (i,j,k) already known.  XY = false / Z =
+// false leave the x/y / z ghosts to the caller (the TMA kernels copy them in
+// a separate pass that interior tiles and planes skip).
+template <bool XY = true, bool Z = true, class S>
 __device__ __forceinline__ void store_at(S* f, const Geom& g, long long o, int i, int j, int k, int gx, int gy,
                                          int gz, S v) {
   f[o] = v;
-  if (gx != NOGHOST) f[o + (gx - i)] = v;
-  if (gy != NOGHOST) f[o + (long long)(gy - j) * g.px] = v;
-  if (gz != NOGHOST) f[o + (long long)(gz - k) * g.pz] = v;
+  if constexpr (XY) {
+    if (gx != NOGHOST) f[o + (gx - i)] = v;
+    if (gy != NOGHOST) f[o + (long long)(gy - j) * g.px] = v;
+  }
+  if constexpr (Z) {
+    if (gz != NOGHOST) f[o + (long long)(gz - k) * g.pz] = v;
+  }
 }
 
 // Deterministic block sum of up to RED_SLOTS values (fixed shuffle and warp
@@ -379,11 +385,11 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
 // offset of (i, j_q, k); gz = ghost_pos(k, nz, R, bcs).  Sites with
 // act[q] false (outside the grid) are computed but neither stored nor
 // reduced, which keeps the arithmetic free of per-site branches.
-template <class S, class C, int R, int KIND, int PY, int NPWX>
+template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true>
 __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)[PY], const S (&pw)[PY][NPWX],
                                             const bool (&act)[PY], int i, const int (&j)[PY], int k,
                                             const long long (&o)[PY], int gz, const ColumnConsts (&cc)[PY],
-                                            double& r_norm, double& r_en, double& r_err) {
+                                            double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr) {
   using T = StageTraits<KIND>;
   const Geom& g = a.g;
   cx<C> lap[PY], c0[PY];
@@ -467,7 +473,7 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
           ns[q] = to_s<S>(cx<C>{base.r + (ar * f[q].r - ai * f[q].i), base.i + (ar * f[q].i + ai * f[q].r)});
         }
-        if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
         if constexpr (KIND == K_RK4_2) {
           // Q = (psi + A)/3 + h/3 k2 in the storage's precision class: Q is
           // rounded to S either way; the last update is the FP64 one above.
@@ -506,7 +512,7 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
         tr = tr + (C)a.b[T::NK] * Kmc.r;
         ti = ti + (C)a.b[T::NK] * Kmc.i;
         ns[q] = to_s<S>(cx<C>{tr, ti});
-        if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
       } else {
         // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
         const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
@@ -525,7 +531,7 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           tr = tr + a.b[T::NK] * Kmd.r;
           ti = ti + a.b[T::NK] * Kmd.i;
           ns[q] = to_s<S>(cx<double>{tr, ti});
-          if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
         } else {
           // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
           // contribute exact zeros and are skipped.
@@ -537,7 +543,7 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
           const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
           ns[q] = to_s<S>(cx<double>{nr, ni});
-          if (act[q]) store_at(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
           const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
           const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
           // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|
@@ -548,6 +554,10 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           if (act[q]) r_err = fmax(r_err, ratio);  // maxval(abs(err/psi_scal)); host divides by eps
         }
       }
+    }
+    if (ns_out) {
+#pragma unroll
+      for (int q = 0; q < PY; ++q) ns_out[q] = ns[q];
     }
     if constexpr (FINAL) {
       if (a.want_norm) {

@@ -238,6 +238,10 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i;
     cc[r] = column_consts(a, i, jr[r], R, act[r]);
   }
+  // does this tile hold a site with an x or y ghost?  Ghosts come from the
+  // index ranges [0, R] and [n-1-R, n-1] of an axis only.
+  const bool xyg = (bx * TX <= R) || (bx * TX + TX - 1 >= g.nx - 1 - R) || (by * TY <= R) ||
+                   (by * TY + TY - 1 >= g.ny - 1 - R);
 
   auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
   S q[PY][2 * R + 1];  // z queue of each owned row: planes k-R .. k+R
@@ -312,7 +316,32 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
 #pragma unroll
         for (int f = 0; f < NPW; ++f) pv[r][f] = pws[f * (TX * TY) + pofs];
       }
-      sites_stage<S, C, R, KIND, PY>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err);
+      constexpr int NPWX = NPW > 0 ? NPW : 1;
+      if constexpr (KIND == K_ENERGY) {
+        sites_stage<S, C, R, KIND, PY, NPWX>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err);
+      } else {
+        // the sites store their own values only; face ghosts are copied
+        // after them, by tiles that touch an x/y face and on the first and
+        // last R + 1 planes only (uniform branches, the site code stays one)
+        S ns[PY];
+        sites_stage<S, C, R, KIND, PY, NPWX, false, false>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err,
+                                                          ns);
+        S* out = (S*)a.out;
+        if (xyg) {
+#pragma unroll
+          for (int r = 0; r < PY; ++r)
+            if (act[r]) {
+              if (cc[r].gx != NOGHOST) out[o[r] + (cc[r].gx - i)] = ns[r];
+              if (cc[r].gy != NOGHOST) out[o[r] + (long long)(cc[r].gy - jr[r]) * g.px] = ns[r];
+            }
+        }
+        if (gz != NOGHOST) {
+          const long long zo = (long long)(gz - k) * g.pz;
+#pragma unroll
+          for (int r = 0; r < PY; ++r)
+            if (act[r]) out[o[r] + zo] = ns[r];
+        }
+      }
     }
 #pragma unroll
     for (int r = 0; r < PY; ++r) {
