@@ -122,6 +122,9 @@ _PROTOS = {
     "gpe_get_site": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
     "gpe_snapshot_begin": (C.c_int, [C.c_void_p, C.c_int32]),
     "gpe_snapshot_wait": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]),
+    "gpe_set_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_get_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "gpe_wait_copies": (C.c_int, [C.c_void_p]),
     "gpe_host_alloc": (C.c_void_p, [C.c_size_t]),
     "gpe_host_free": (None, [C.c_void_p]),
     "gpe_slab_nccl_id": (C.c_int, [C.c_void_p]),

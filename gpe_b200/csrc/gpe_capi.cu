@@ -112,6 +112,15 @@ struct gpe_handle {
   // (the stage arguments, dt included, are baked into the graph)
   cudaGraphExec_t step_graph = nullptr;
   double graph_dr = 0, graph_di = 0;
+  // asynchronous state copies (gpe_set_state_async / gpe_get_state_async):
+  // host <-> staging transfers on a copy stream, pack/unpack on the solve's
+  // stream, ordered by events so transfers overlap the steps around them
+  cudaStream_t cp_st = nullptr;   // host -> device transfers
+  cudaStream_t cp2_st = nullptr;  // device -> host transfers (a stream each, so neither queues behind the other)
+  void *in_stage = nullptr, *out_stage = nullptr;
+  size_t in_cap = 0, out_cap = 0;
+  cudaEvent_t ev_packed = nullptr, ev_in = nullptr, ev_unpacked = nullptr, ev_out = nullptr;
+  bool copies_pending = false;
 };
 
 struct gpe_slab_hub {
@@ -815,6 +824,15 @@ void gpe_destroy(gpe_handle* h) {
   if (h->fft_work) cudaFree(h->fft_work);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+  for (cudaStream_t c : {h->cp_st, h->cp2_st})
+    if (c) {
+      cudaStreamSynchronize(c);
+      cudaStreamDestroy(c);
+    }
+  for (cudaEvent_t e : {h->ev_packed, h->ev_in, h->ev_unpacked, h->ev_out})
+    if (e) cudaEventDestroy(e);
+  if (h->in_stage) cudaFree(h->in_stage);
+  if (h->out_stage) cudaFree(h->out_stage);
   if (h->snap_st) {
     cudaStreamSynchronize(h->snap_st);
     cudaStreamDestroy(h->snap_st);
@@ -957,9 +975,84 @@ int gpe_step(gpe_handle* h, int64_t nsteps, gpe_step_info* io) { return step_imp
 
 int gpe_step_async(gpe_handle* h, int64_t nsteps, gpe_step_info* io) { return step_impl(h, nsteps, io, false); }
 
+// copy stream, staging buffers and events of the asynchronous state copies
+static int ensure_async_copies(gpe_handle* h, size_t bytes) {
+  if (!h->cp_st) {
+    CU(h, cudaStreamCreateWithFlags(&h->cp_st, cudaStreamNonBlocking));
+    CU(h, cudaStreamCreateWithFlags(&h->cp2_st, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&h->ev_packed, &h->ev_in, &h->ev_unpacked, &h->ev_out})
+      CU(h, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    // record every event once so that the first waits on them are no-ops
+    for (cudaEvent_t e : {h->ev_packed, h->ev_unpacked}) CU(h, cudaEventRecord(e, h->st));
+    CU(h, cudaEventRecord(h->ev_in, h->cp_st));
+    CU(h, cudaEventRecord(h->ev_out, h->cp2_st));
+  }
+  if (h->in_cap < bytes || h->out_cap < bytes) {
+    CU(h, cudaStreamSynchronize(h->st));
+    CU(h, cudaStreamSynchronize(h->cp_st));
+    CU(h, cudaStreamSynchronize(h->cp2_st));
+    if (h->in_stage) cudaFree(h->in_stage);
+    if (h->out_stage) cudaFree(h->out_stage);
+    h->in_stage = h->out_stage = nullptr;
+    h->in_cap = h->out_cap = 0;
+    CU(h, cudaMalloc(&h->in_stage, bytes));
+    CU(h, cudaMalloc(&h->out_stage, bytes));
+    h->in_cap = h->out_cap = bytes;
+  }
+  return GPE_OK;
+}
+
+int gpe_set_state_async(gpe_handle* h, const void* psi, int32_t dtype) {
+  if (!h || !psi) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  const size_t bytes = interior_bytes(h, dtype);
+  if (int rc = ensure_async_copies(h, bytes)) return rc;
+  // the previous pack must be done with the input staging buffer
+  CU(h, cudaStreamWaitEvent(h->cp_st, h->ev_packed, 0));
+  CU(h, cudaMemcpyAsync(h->in_stage, psi, bytes, cudaMemcpyHostToDevice, h->cp_st));
+  CU(h, cudaEventRecord(h->ev_in, h->cp_st));
+  CU(h, cudaStreamWaitEvent(h->st, h->ev_in, 0));
+  if (int rc = pack_from_device(h, h->in_stage, dtype)) return rc;
+  CU(h, cudaEventRecord(h->ev_packed, h->st));
+  h->copies_pending = true;
+  return GPE_OK;
+}
+
+int gpe_get_state_async(gpe_handle* h, void* psi, int32_t dtype) {
+  if (!h || !psi) return fail(h, GPE_ERR_BADARG, "null argument");
+  if (int rc = check_dtype(h, dtype)) return rc;
+  CU(h, cudaSetDevice(h->dev));
+  const size_t bytes = interior_bytes(h, dtype);
+  if (int rc = ensure_async_copies(h, bytes)) return rc;
+  // the previous transfer must be done with the output staging buffer
+  CU(h, cudaStreamWaitEvent(h->st, h->ev_out, 0));
+  if (int rc = unpack_to_device(h, h->out_stage, dtype)) return rc;
+  CU(h, cudaEventRecord(h->ev_unpacked, h->st));
+  CU(h, cudaStreamWaitEvent(h->cp2_st, h->ev_unpacked, 0));
+  CU(h, cudaMemcpyAsync(psi, h->out_stage, bytes, cudaMemcpyDeviceToHost, h->cp2_st));
+  CU(h, cudaEventRecord(h->ev_out, h->cp2_st));
+  h->copies_pending = true;
+  return GPE_OK;
+}
+
+int gpe_wait_copies(gpe_handle* h) {
+  if (!h) return GPE_ERR_BADARG;
+  if (!h->cp_st) return GPE_OK;
+  CU(h, cudaSetDevice(h->dev));
+  CU(h, cudaStreamWaitEvent(h->st, h->ev_out, 0));
+  CU(h, cudaStreamWaitEvent(h->st, h->ev_in, 0));
+  return GPE_OK;
+}
+
 int gpe_sync(gpe_handle* h) {
   if (!h) return GPE_ERR_BADARG;
   CU(h, cudaSetDevice(h->dev));
+  if (h->cp_st) {
+    CU(h, cudaStreamSynchronize(h->cp_st));
+    CU(h, cudaStreamSynchronize(h->cp2_st));
+    h->copies_pending = false;
+  }
   CU(h, cudaStreamSynchronize(h->st));
   if (h->prof) prof_resolve(h);
   return check_status(h);

@@ -168,6 +168,24 @@ class Solver:
         buf = (C.c_char * n.value).from_address(ptr.value)
         return np.frombuffer(buf, dtype=self._snap_dtype).reshape(self.shape).copy()
 
+    def set_state_async(self, psi: np.ndarray) -> None:
+        """gpe_set_state_async: psi must be page-locked (gpe_b200._lib.pinned_empty),
+        C-contiguous, and left untouched until sync()."""
+        if psi.shape != self.shape or not psi.flags.c_contiguous:
+            raise ValueError(f"psi must be a C-contiguous array of shape {self.shape}")
+        code = L.GPE_C64 if psi.dtype == np.complex64 else L.GPE_C128
+        _check(self.lib, self.h, self.lib.gpe_set_state_async(self.h, psi.ctypes.data, code))
+
+    def get_state_async(self, out: np.ndarray) -> None:
+        """gpe_get_state_async into a page-locked array; valid after sync()."""
+        if out.shape != self.shape or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous array of shape {self.shape}")
+        code = L.GPE_C64 if out.dtype == np.complex64 else L.GPE_C128
+        _check(self.lib, self.h, self.lib.gpe_get_state_async(self.h, out.ctypes.data, code))
+
+    def wait_copies(self) -> None:
+        _check(self.lib, self.h, self.lib.gpe_wait_copies(self.h))
+
     def set_ic(self, spec) -> None:
         """Generate the initial state on the device (see ic.device_spec)."""
         _check(self.lib, self.h, self.lib.gpe_set_ic(self.h, C.byref(spec)))

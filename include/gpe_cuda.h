@@ -132,6 +132,18 @@ int gpe_step(gpe_handle* h, int64_t nsteps, gpe_step_info* io);
 int gpe_step_async(gpe_handle* h, int64_t nsteps, gpe_step_info* io);
 int gpe_sync(gpe_handle* h);
 
+/* Asynchronous forms of gpe_set_state / gpe_get_state for a pipeline of
+ * solves: the host<->device transfer runs on the handle's copy stream
+ * through device staging buffers, ordered with the handle's stream by
+ * events, so the transfers of one solve overlap the steps of the next.
+ * Both return at once.  psi must be page-locked (gpe_host_alloc) and must
+ * not be touched until gpe_sync returns.  gpe_wait_copies orders the
+ * handle's stream after every transfer issued so far (no host wait), e.g.
+ * before recording a timing event; gpe_sync waits for the transfers too. */
+int gpe_set_state_async(gpe_handle* h, const void* psi, int32_t dtype);
+int gpe_get_state_async(gpe_handle* h, void* psi, int32_t dtype);
+int gpe_wait_copies(gpe_handle* h);
+
 /* get_norm (src/variables.f90:554-576) of the current state. */
 int gpe_norm(gpe_handle* h, double* norm);
 /* energy (src/variables.f90:580-604), un-normalised: io.f90:202 divides the

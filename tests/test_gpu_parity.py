@@ -278,3 +278,28 @@ def test_grid_below_the_minimum_is_rejected(gpu):
     with pytest.raises(L.GpeError) as e:
         Solver(rp)
     assert e.value.code == L.GPE_ERR_BADARG
+
+
+def test_async_state_copies_pipeline(gpu):
+    """gpe_set_state_async / gpe_get_state_async in a pipeline of three
+    solves from different inputs: each result equals the synchronous path's,
+    although transfers overlap the neighbouring solves' steps."""
+    rp = c1_params(nx=40, ny=36, nz=34, xr=9.75, yr=8.75, zr=8.25)
+    ins = [L.pinned_empty((34, 36, 40), np.complex128) for _ in range(3)]
+    outs = [L.pinned_empty((34, 36, 40), np.complex128) for _ in range(3)]
+    for q, a in enumerate(ins):
+        a[...] = ic.vortex_ring(rp, "xy", r0=2.0 + q)
+    ref = []
+    s = Solver(rp)
+    for a in ins:
+        s.set_state(a)
+        s.solver(6)
+        ref.append(s.get_state())
+    for a, o in zip(ins, outs):
+        s.set_state_async(a)
+        s.solver(6, wait=False)
+        s.get_state_async(o)
+    s.sync()
+    for o, r in zip(outs, ref):
+        np.testing.assert_array_equal(o, r)
+    s.close()
