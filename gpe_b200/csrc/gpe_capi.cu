@@ -389,16 +389,16 @@ int enqueue_fixed_step(gpe_handle* h, double dr, double di, bool energy, bool no
     if (energy && finalize_into(h, h->part_a, 0)) return GPE_ERR_CUDA;
     a.want_energy = 0;
     a.partials = nullptr;
-    // s2: k2 = f(A); B = psi + dt/2 k2; Q = (psi + A)/3 + dt/3 k2
+    // s2: k2 = f(A); B = psi + dt/2 k2; Q = (psi + A) + dt k2
     a.in = A; a.psi = psi; a.out = B; a.acc = Q;
     a.cf_r[0] = 0.5 * dr; a.cf_i[0] = 0.5 * di;
-    a.cf_r[1] = dr / 3.0; a.cf_i[1] = di / 3.0;
+    a.cf_r[1] = dr; a.cf_i[1] = di;
     CU(h, launch(h, K_RK4_2, a));
     // s3: k3 = f(B); A = psi + dt k3
     a.in = B; a.out = A;
     a.cf_r[0] = dr; a.cf_i[0] = di;
     CU(h, launch(h, K_RK4_3, a));
-    // s4: k4 = f(A); psi = Q + A/3 + dt/6 k4 (psi itself is not read)
+    // s4: k4 = f(A); psi = (Q + A)/3 + dt/6 k4 (psi itself is not read)
     a.in = A; a.psi = nullptr; a.out = psi;
     a.cf_r[0] = dr / 6.0; a.cf_i[0] = di / 6.0;
     a.want_norm = norm;

@@ -443,18 +443,19 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
       if constexpr (KIND == K_EULER || KIND == K_RK2_1 || KIND == K_RK4_1 || KIND == K_RK2_2 ||
                     KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) {
         // out = base + cf0 * f, with base = psi_n (pv), the stencil centre,
-        // or for RK4 stage 4 the accumulator plus a third of the centre.
-        // Outputs that are a new psi (Euler, RK2 stage 2, RK4 stage 4) are
-        // formed in FP64; intermediate stage inputs in the stencil's compute
-        // type C (identical to FP64 when C = double).
+        // or for RK4 stage 4 a third of (accumulator + centre).  Outputs that
+        // are a new psi (Euler, RK2 stage 2, RK4 stage 4) are formed in FP64;
+        // intermediate stage inputs in the stencil's compute type C
+        // (identical to FP64 when C = double).
         //
         // RK4 runs in a reduced-traffic form of classical RK4 (h = dt):
         //   s1: A = psi + h/2 k1
-        //   s2: B = psi + h/2 k2,  Q = (psi + A)/3 + h/3 k2  (= 2psi/3 + h/6 k1 + h/3 k2)
+        //   s2: B = psi + h/2 k2,  Q = (psi + A) + h k2  (= 2psi + h/2 k1 + h k2)
         //   s3: A = psi + h k3
-        //   s4: psi' = Q + A/3 + h/6 k4  (= psi + h (k1/6 + k2/3 + k3/3 + k4/6))
+        //   s4: psi' = (Q + A)/3 + h/6 k4  (= psi + h (k1/6 + k2/3 + k3/3 + k4/6))
         // so that stage 1 reads 1 field, stage 3 reads 2 and stage 4 reads 2
-        // (solve.f90:124-148 keeps k1..k4; the sum is the same).
+        // (solve.f90:124-148 keeps k1..k4; the sum is the same).  The only
+        // division by 3 sits in the FP64 update of stage 4.
         constexpr double THIRD = 1.0 / 3.0;
         if constexpr (FINAL || sizeof(C) == sizeof(double)) {
           cx<double> base;
@@ -462,7 +463,7 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
             base = to_c<double>(pv);
           } else if constexpr (KIND == K_RK4_4) {
             const cx<double> qv = to_c<double>(av);
-            base = cx<double>{qv.r + THIRD * cr, qv.i + THIRD * ci};
+            base = cx<double>{(qv.r + cr) * THIRD, (qv.i + ci) * THIRD};
           } else {
             base = cx<double>{cr, ci};
           }
@@ -475,21 +476,19 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
         }
         if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
         if constexpr (KIND == K_RK4_2) {
-          // Q = (psi + A)/3 + h/3 k2 in the storage's precision class: Q is
-          // rounded to S either way; the last update is the FP64 one above.
-          // The third is taken in FP64 also for C = float: a C-rounded 1/3
-          // would scale psi by a biased factor every step.
+          // Q = (psi + A) + h k2 in the stencil's compute type: Q is rounded
+          // to S either way, and no third enters here (a C-rounded 1/3 would
+          // scale psi by a biased factor every step); cf1 = h
           S qs;
           if constexpr (sizeof(C) == sizeof(double)) {
             const cx<double> pd = to_c<double>(pv);
             const cx<double> t1 = cmuld(a.cf_r[1], a.cf_i[1], fd);
-            qs = to_s<S>(cx<double>{(pd.r + cr) * THIRD + t1.r, (pd.i + ci) * THIRD + t1.i});
+            qs = to_s<S>(cx<double>{(pd.r + cr) + t1.r, (pd.i + ci) + t1.i});
           } else {
             const cx<C> pc = to_c<C>(pv);
             const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
-            const double qr = ((double)pc.r + cr) * THIRD + (double)(br * f[q].r - bi * f[q].i);
-            const double qi = ((double)pc.i + ci) * THIRD + (double)(br * f[q].i + bi * f[q].r);
-            qs = to_s<S>(cx<double>{qr, qi});
+            qs = to_s<S>(cx<C>{(pc.r + c0[q].r) + (br * f[q].r - bi * f[q].i),
+                               (pc.i + c0[q].i) + (br * f[q].i + bi * f[q].r)});
           }
           if (act[q]) ((S*)a.acc)[o[q]] = qs;
         }

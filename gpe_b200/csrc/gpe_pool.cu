@@ -284,7 +284,7 @@ BatchStage make_stage(gpe_pool* P, Solve* s, int kind, int fin, int fout, std::i
 
 // RK4 tables: 4 stages (fields psi=0, A=1, B=2, Q=3) of the reduced-traffic
 // RK4 form of site_stage: A = psi + h/2 k1; B = psi + h/2 k2,
-// Q = (psi + A)/3 + h/3 k2; A = psi + h k3; psi = Q + A/3 + h/6 k4
+// Q = (psi + A) + h k2; A = psi + h k3; psi = (Q + A)/3 + h/6 k4
 void rk4_tables(gpe_pool* P, Solve* s, BatchStage* t4) {
   const double dr = s->dr, di = s->di;
   BatchStage b = make_stage(P, s, K_RK4_1, 0, 1, {});
@@ -294,7 +294,7 @@ void rk4_tables(gpe_pool* P, Solve* s, BatchStage* t4) {
   b.args.psi = s->f[0];
   b.args.acc = s->f[3];
   b.args.cf_r[0] = 0.5 * dr; b.args.cf_i[0] = 0.5 * di;
-  b.args.cf_r[1] = dr / 3.0; b.args.cf_i[1] = di / 3.0;
+  b.args.cf_r[1] = dr; b.args.cf_i[1] = di;
   t4[1] = b;
   b = make_stage(P, s, K_RK4_3, 2, 1, {0});
   b.args.psi = s->f[0];
