@@ -1,9 +1,11 @@
 // C ABI of the B200 Gross-Pitaevskii time-stepper (include/gpe_cuda.h).
 //
-// One handle = one solve: ghost-padded device fields, per-axis tables, a
-// stream, reduction buffers.  gpe_step() enqueues one fused stage kernel per
-// Runge-Kutta stage; the time bookkeeping follows the reference's solver()
-// routines (src/solve.f90:57-244) on the host, in FP64.
+// One handle = one solve (or one z-slab of a decomposed solve): ghost-padded
+// device fields, per-axis tables, a stream, reduction buffers.  gpe_step()
+// enqueues one fused stage kernel per Runge-Kutta stage (steps without
+// reductions as a replayed graph of one step); the time bookkeeping follows
+// the reference's solver() routines (src/solve.f90:57-244) on the host, in
+// FP64.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
