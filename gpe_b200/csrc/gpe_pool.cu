@@ -29,11 +29,11 @@
 
 namespace gpe {
 cudaError_t launch_batch_f64(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                             int nitems, double* partials, int* occupancy);
+                             const int* order, int nitems, int* queue, double* partials, int* occupancy);
 cudaError_t launch_batch_f32(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                             int nitems, double* partials, int* occupancy);
+                             const int* order, int nitems, int* queue, double* partials, int* occupancy);
 cudaError_t launch_batch_f32x(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                              int nitems, double* partials, int* occupancy);
+                              const int* order, int nitems, int* queue, double* partials, int* occupancy);
 }  // namespace gpe
 
 using namespace gpe;
@@ -158,12 +158,15 @@ struct Class {
   bool dirty = true;
   DevBuf<BatchStage> tab;   // [stage][solve]
   DevBuf<BatchItem> items;
+  DevBuf<int> order;        // item indices, largest items first (the work queue's order)
+  DevBuf<int> queue;        // one work-queue counter per stage launch, zeroed before each step
   DevBuf<int> first;        // [solve + 1] item ranges
   DevBuf<double> part;      // [item][RED_SLOTS]
   DevBuf<double> res;       // [solve][RED_SLOTS]
   HostPinned<BatchStage> htab;
   HostPinned<double> hres;
   std::vector<BatchItem> hitems;
+  std::vector<int> horder;
   std::vector<int> hfirst;
   int nitems = 0;
   cudaGraph_t graph = nullptr;
@@ -219,17 +222,18 @@ int cmode_of(const gpe_params& p) {
 }
 
 cudaError_t launch_batch(int cmode, int kind, int grid, cudaStream_t st, const BatchStage* tab,
-                         const BatchItem* items, int nitems, double* partials, int* occ) {
+                         const BatchItem* items, const int* order, int nitems, int* queue, double* partials,
+                         int* occ) {
   switch (cmode) {
-    case CM_F64: return launch_batch_f64(kind, grid, st, tab, items, nitems, partials, occ);
-    case CM_F32: return launch_batch_f32(kind, grid, st, tab, items, nitems, partials, occ);
-    default: return launch_batch_f32x(kind, grid, st, tab, items, nitems, partials, occ);
+    case CM_F64: return launch_batch_f64(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
+    case CM_F32: return launch_batch_f32(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
+    default: return launch_batch_f32x(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
   }
 }
 
 int grid_for(int cmode, int kind, int nitems) {
   int occ = 0;
-  launch_batch(cmode, kind, 0, nullptr, nullptr, nullptr, 0, nullptr, &occ);
+  launch_batch(cmode, kind, 0, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, &occ);
   return std::max(1, std::min(nitems, occ));
 }
 
@@ -352,13 +356,29 @@ int build_items(gpe_pool* P, Class& c, const std::vector<Solve*>& sv) {
     c.hfirst.push_back((int)c.hitems.size());
   }
   c.nitems = (int)c.hitems.size();
+  // work-queue order: largest items first (planes x sites in the tile, plus
+  // the 2R halo planes every item reads), ties in item order
+  std::vector<double> cost(c.hitems.size());
+  for (size_t w = 0; w < c.hitems.size(); ++w) {
+    const BatchItem& it = c.hitems[w];
+    const Solve* s = sv[it.solve];
+    const int m = std::min(s->zc, s->g.nz - it.bz * s->zc);
+    const int cols = std::min(32, s->g.nx - it.bx * 32), rows = std::min(8, s->g.ny - it.by * 8);
+    cost[w] = (double)(m + 2 * s->R) * cols * rows;
+  }
+  c.horder.resize(c.hitems.size());
+  for (size_t w = 0; w < c.horder.size(); ++w) c.horder[w] = (int)w;
+  std::stable_sort(c.horder.begin(), c.horder.end(), [&](int u, int v) { return cost[u] > cost[v]; });
   PCU(P, c.items.ensure(c.hitems.size()));
+  PCU(P, c.order.ensure(c.horder.size()));
+  PCU(P, c.queue.ensure(8));
   PCU(P, c.first.ensure(c.hfirst.size()));
   PCU(P, c.part.ensure(c.hitems.size() * RED_SLOTS));
   PCU(P, c.res.ensure(sv.size() * RED_SLOTS));
   PCU(P, c.hres.ensure(sv.size() * RED_SLOTS));
   PCU(P, cudaMemcpyAsync(c.items.p, c.hitems.data(), c.hitems.size() * sizeof(BatchItem), cudaMemcpyHostToDevice,
                          c.st));
+  PCU(P, cudaMemcpyAsync(c.order.p, c.horder.data(), c.horder.size() * sizeof(int), cudaMemcpyHostToDevice, c.st));
   PCU(P, cudaMemcpyAsync(c.first.p, c.hfirst.data(), c.hfirst.size() * sizeof(int), cudaMemcpyHostToDevice, c.st));
   return GPE_OK;
 }
@@ -403,10 +423,10 @@ int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
     // capture one RK4 step of the whole class
     PCU(P, cudaStreamSynchronize(c.st));
     PCU(P, cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(c.queue.p, 0, 4 * sizeof(int), c.st);
     for (int m = 0; m < 4 && e == cudaSuccess; ++m)
-      e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)m * ns, c.items.p, c.nitems,
-                       m == 3 ? c.part.p : nullptr, nullptr);
+      e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)m * ns, c.items.p, c.order.p, c.nitems,
+                       c.queue.p + m, m == 3 ? c.part.p : nullptr, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(c.st, &g);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -462,9 +482,10 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
     for (int m = 0; m < 6; ++m) c.htab.p[(size_t)m * ns + q] = t6[m];
   }
   PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
+  PCU(P, cudaMemsetAsync(c.queue.p, 0, 6 * sizeof(int), c.st));
   for (int m = 0; m < 6; ++m)
     PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), c.st, c.tab.p + (size_t)m * ns,
-                        c.items.p, c.nitems, m == 5 ? c.part.p : nullptr, nullptr));
+                        c.items.p, c.order.p, c.nitems, c.queue.p + m, m == 5 ? c.part.p : nullptr, nullptr));
   k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
   PCU(P, cudaGetLastError());
   PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));
@@ -787,6 +808,8 @@ void gpe_pool_destroy(gpe_pool* P) {
       }
       c.tab.free();
       c.items.free();
+      c.order.free();
+      c.queue.free();
       c.first.free();
       c.part.free();
       c.res.free();

@@ -126,22 +126,24 @@ static cudaError_t batch_setup(int* occupancy) {
 
 template <class S, class C, int K>
 static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                                    int nitems, double* partials) {
+                                    const int* order, int nitems, int* queue, double* partials) {
   using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
   cudaError_t e = batch_setup<S, C, K>(nullptr);
   if (e != cudaSuccess) return e;
-  k_stage_batch<S, C, K, 8, BATCH_PY><<<grid, dim3(32, 8 / BATCH_PY), LY::SMEM, st>>>(tab, items, nitems, partials);
+  k_stage_batch<S, C, K, 8, BATCH_PY><<<grid, dim3(32, 8 / BATCH_PY), LY::SMEM, st>>>(tab, items, order, nitems,
+                                                                                        queue, partials);
   return cudaGetLastError();
 }
 
 template <class S, class C>
 static cudaError_t launch_batch_impl(int kind, int grid, cudaStream_t st, const BatchStage* tab,
-                                     const BatchItem* items, int nitems, double* partials, int* occupancy) {
+                                     const BatchItem* items, const int* order, int nitems, int* queue,
+                                     double* partials, int* occupancy) {
   switch (kind) {
 #define GPE_BCASE(K)                                                       \
   case K:                                                                  \
     if (grid <= 0) return batch_setup<S, C, K>(occupancy);               \
-    return launch_batch_one<S, C, K>(grid, st, tab, items, nitems, partials);
+    return launch_batch_one<S, C, K>(grid, st, tab, items, order, nitems, queue, partials);
     GPE_BCASE(K_RK4_1)
     GPE_BCASE(K_RK4_2)
     GPE_BCASE(K_RK4_3)
@@ -178,7 +180,8 @@ static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStr
     return launch_stage_tma_impl<S, C>(kind, R, ty, grid, st, m, a);                                    \
   }                                                                                                     \
   cudaError_t launch_batch_##TAG(int kind, int grid, cudaStream_t st, const BatchStage* tab,            \
-                                 const BatchItem* items, int nitems, double* partials, int* occupancy) { \
-    return launch_batch_impl<S, C>(kind, grid, st, tab, items, nitems, partials, occupancy);            \
+                                 const BatchItem* items, const int* order, int nitems, int* queue,     \
+                                 double* partials, int* occupancy) {                                   \
+    return launch_batch_impl<S, C>(kind, grid, st, tab, items, order, nitems, queue, partials, occupancy); \
   }                                                                                                     \
   }

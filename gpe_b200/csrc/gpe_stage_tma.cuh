@@ -387,12 +387,14 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
 // ---------------------------------------------------------------------------
 // Batched, persistent stage kernel: many independent solves (any sizes, BCs,
 // orders 2 and 4) advanced by one launch per stage.  Work item w = tile
-// (bx, by, bz) of solve items[w].solve; CTA b processes items b, b + grid,
-// b + 2 grid, ...  Per-solve stage arguments and tensor maps live in a
-// device table; each CTA copies the item's arguments to shared memory.
-// Reductions go to per-item partials, summed per solve by k_finalize_ranges
-// in a fixed order, so a solve's results do not depend on what else is in
-// the batch.
+// (bx, by, bz) of solve items[w].solve.  CTAs take items from a work queue:
+// an atomic counter (zero at launch) indexes `order`, which lists the items
+// largest first, so the launch ends with small items spread over all CTAs
+// instead of a few CTAs finishing a long tail.  Per-solve stage arguments
+// and tensor maps live in a device table.  Reductions go to per-item
+// partials (indexed by w, whichever CTA runs the item), summed per solve by
+// k_finalize_ranges in a fixed order, so a solve's results depend neither on
+// what else is in the batch nor on the schedule.
 // ---------------------------------------------------------------------------
 struct alignas(64) BatchStage {
   TmaMaps maps;
@@ -405,15 +407,24 @@ struct BatchItem {
 
 template <class S, class C, int KIND, int TY, int PY>
 __global__ void __launch_bounds__(32 * TY / PY) k_stage_batch(const BatchStage* __restrict__ tab,
-                                                         const BatchItem* __restrict__ items, int nitems,
-                                                         double* partials) {
+                                                         const BatchItem* __restrict__ items,
+                                                         const int* __restrict__ order, int nitems,
+                                                         int* queue, double* partials) {
   using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
+  __shared__ int s_w[2];  // item taken from the queue, double-buffered by turn parity
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   const int tid = threadIdx.y * 32 + threadIdx.x;
   int fenced = -1;  // solve whose tensor maps thread 0 has acquired (they do not change within a launch)
-  for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+  for (int turn = 0;; ++turn) {
+    if (tid == 0) {
+      const int q = atomicAdd(queue, 1);
+      s_w[turn & 1] = q < nitems ? order[q] : -1;
+    }
+    __syncthreads();
+    const int w = s_w[turn & 1];
+    if (w < 0) break;
     const BatchItem it = items[w];
     const BatchStage* bs = tab + it.solve;
     if (tid == 0 && it.solve != fenced) {
