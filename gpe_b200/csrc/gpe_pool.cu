@@ -608,7 +608,10 @@ static int pool_submit_impl(gpe_pool* P, const gpe_params* prm, const void* psi0
   s->cmode = cmode_of(*prm);
   s->fam = prm->scheme == GPE_RK45 ? FAM_RK45 : FAM_RK4;
   s->nf = scheme_fields(prm->scheme);
-  s->zc = prm->tile_zc > 0 ? std::min(prm->tile_zc, prm->nz) : default_zc(s->g);
+  // z planes per work item: the caller's (autotuned) choice, else a batch
+  // default.  In a batch the other solves fill the GPU, so items can be long
+  // (fewer z-halo re-reads per plane) instead of many.
+  s->zc = prm->tile_zc > 0 ? std::min(prm->tile_zc, prm->nz) : std::min(prm->nz, prm->nz <= 48 ? 16 : 32);
   s->ntx = (prm->nx + 31) / 32;
   s->nty = (prm->ny + 7) / 8;
   s->ntz = (prm->nz + s->zc - 1) / s->zc;

@@ -405,8 +405,18 @@ struct BatchItem {
   int solve, bx, by, bz;
 };
 
+// CTAs per SM the batched RK4 kernels' registers are fitted to.  The R = 1
+// and R = 2 item bodies share one kernel, so unbounded they take 96-128
+// registers at FP32 and 124-154 at FP64; bounded to 6 CTAs of 128 threads
+// (80 registers) at FP32 and 4 (128) at FP64 they spill a few words and run
+// 2-4 % faster on a batch of uneven solves.
+template <class C, int KIND>
+__host__ __device__ constexpr int batch_min_blocks() {
+  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) ? (sizeof(C) == 4 ? 6 : 4) : 1;
+}
+
 template <class S, class C, int KIND, int TY, int PY>
-__global__ void __launch_bounds__(32 * TY / PY) k_stage_batch(const BatchStage* __restrict__ tab,
+__global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k_stage_batch(const BatchStage* __restrict__ tab,
                                                          const BatchItem* __restrict__ items,
                                                          const int* __restrict__ order, int nitems,
                                                          int* queue, double* partials) {
