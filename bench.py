@@ -280,22 +280,21 @@ C4_STEPS = 500
 C4_SHORT = 200
 
 
-def batched_leg(args, torch):
-    """64 independent solves in one pool: cubic sizes uniform in
+def c4_mix(storage: str = "c64", tuned: bool = True):
+    """The 64 uneven solves of the batched workload: cubic sizes uniform in
     {32, 48, ..., 160}, periodic/reflective and 2nd/4th order mixed (seeded),
-    RK4 dt = 0.01, 500 steps, ring (r0 in [2,6]) / random-phase (cutoff in
-    [1,2]) initial states alternating, complex64 storage with FP64
-    reductions, tile_zc per size from the autotuner.  Timed on the host clock
-    from the first submission to the last retired result (state upload and
-    download included); latencies are per solve, all submitted at t = 0."""
+    RK4 dt = 0.01, eqn 4, ring (r0 in [2,6]) / random-phase (cutoff in
+    [1,2]) initial states alternating.  tuned: tile_zc per size from the
+    autotuner (measured on a cache miss), else the pool's default.  Returns
+    [(params, page-locked input, page-locked result buffer)] and the cache."""
     from gpe_b200 import _lib as L
     from gpe_b200 import autotune
     from gpe_b200 import ic
-    from gpe_b200.pool import Pool
     from gpe_b200.solver import RunParams
 
     rng = np.random.default_rng(64)
-    cache = autotune.load_cache()
+    cache = autotune.load_cache() if tuned else {}
+    dt = np.complex64 if storage == "c64" else np.complex128
     solves = []
     for k in range(64):
         n = int(rng.choice(np.arange(32, 161, 16)))
@@ -303,14 +302,27 @@ def batched_leg(args, torch):
         r0, kc = float(rng.uniform(2, 6)), float(rng.uniform(1, 2))
         h = 0.25 * (n - 1)
         rp = RunParams(nx=n, ny=n, nz=n, xr=h, yr=h, zr=h, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=bcs,
-                       order=order, g=1.0, mu=1.0, storage="c64",
-                       tile_zc=autotune.best_zc(n, order, "c64", cache))
+                       order=order, g=1.0, mu=1.0, storage=storage,
+                       tile_zc=autotune.best_zc(n, order, storage, cache) if tuned else 0)
         psi = ic.vortex_ring(rp, "xy", r0=r0) if k % 2 == 0 else ic.random_phase(rp, seed=k, kc=kc)
         # the caller's input and result buffers: page-locked, allocated once
-        host = L.pinned_empty(psi.shape, np.complex64)
+        host = L.pinned_empty(psi.shape, dt)
         host[...] = psi
-        solves.append((rp, host, L.pinned_empty(psi.shape, np.complex64)))
-    autotune.save_cache(cache)
+        solves.append((rp, host, L.pinned_empty(psi.shape, dt)))
+    if tuned:
+        autotune.save_cache(cache)
+    return solves, cache
+
+
+def batched_leg(args, torch):
+    """The c4_mix solves in one pool, complex64 storage with FP64
+    reductions, 500 steps, tile_zc per size from the autotuner.  Timed on the
+    host clock from the first submission to the last retired result (state
+    upload and download included); latencies are per solve, all submitted at
+    t = 0."""
+    from gpe_b200.pool import Pool
+
+    solves, cache = c4_mix("c64", tuned=True)
     budget = sum(Pool.solve_bytes(rp) for rp, _, _ in solves) + (256 << 20)
     sites = sum(rp.nx * rp.ny * rp.nz for rp, _, _ in solves)
 
@@ -348,6 +360,20 @@ def batched_leg(args, torch):
             "timing": "value: host clock, first submit to last result, uploads/downloads included (the caller's "
                       "states and result buffers in page-locked host memory); stepping_rate: host clock around "
                       f"{C4_SHORT} steps of the whole mix resident on the device (synchronised both sides)"}
+
+
+def ncu_batch_case(args) -> int:
+    """Profiling target for the batched kernel: the c4_mix solves (storage
+    --storage, pool default z-chunks) submitted to one pool, 12 RK4 steps."""
+    from gpe_b200.pool import Pool
+
+    solves, _ = c4_mix(args.storage, tuned=False)
+    pool = Pool(sum(Pool.solve_bytes(rp) for rp, _, _ in solves) + (256 << 20))
+    for k, (rp, psi, out) in enumerate(solves):
+        assert pool.submit(rp, psi, 12, k, out=out)
+    pool.run_all()
+    pool.close()
+    return 0
 
 
 def run_serving(args) -> int:
@@ -392,12 +418,17 @@ def main() -> int:
     ap.add_argument("--requests", type=int, default=40, help="--serving: requests in the sample")
     ap.add_argument("--storage", default="c128", choices=["c128", "c64"],
                     help="storage of the --ncu-case / --quick workload")
+    ap.add_argument("--batch", action="store_true",
+                    help="with --ncu-case: the 64 uneven solves of the batched workload in one pool "
+                         "(pool default z-chunks), 12 RK4 steps")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
     if args.serving:
         return run_serving(args)
+    if args.ncu_case and args.batch:
+        return ncu_batch_case(args)
 
     import torch
 

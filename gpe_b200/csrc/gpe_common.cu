@@ -85,22 +85,28 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Tensor maps of one ghost-padded field: rank 3 over (2*px scalars, ny+4
-// rows, nz+4 planes); box = halo'd stencil tile or plain point-wise tile.
+// Tensor maps of one ghost-padded field: rank 3 over (x scalars, ny+4 rows,
+// nz+4 planes); box = halo'd stencil tile or plain point-wise tile.  The x
+// extent ends at the last column a box's consumer can use -- the ghost
+// column x = nx+1 for the stencil, x = nx-1 for point-wise tiles -- so the
+// TMA unit zero-fills the rest of a partial tile instead of reading the
+// row padding from HBM (only lanes outside the grid see those zeros).  No
+// L2 sector promotion: a box row is fetched as the sectors it covers.
 bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw) {
   auto enc = tensor_map_encoder();
   if (!enc) return false;
   const CUtensorMapDataType dt = esz == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-  const cuuint64_t dims[3] = {(cuuint64_t)(2 * g.px), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
+  const cuuint64_t dims_h[3] = {(cuuint64_t)(2 * (g.xoff + g.nx + 2)), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
+  const cuuint64_t dims_p[3] = {(cuuint64_t)(2 * (g.xoff + g.nx)), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
   const cuuint64_t strides[2] = {(cuuint64_t)(g.px * esz), (cuuint64_t)(g.pz * esz)};
   const cuuint32_t estr[3] = {1, 1, 1};
   const cuuint32_t box_h[3] = {(cuuint32_t)(2 * tma_stencil_w()), (cuuint32_t)tma_stencil_h(8, R), 1};
   const cuuint32_t box_p[3] = {(cuuint32_t)(2 * TMA_TX), 8, 1};
-  if (enc(halo, dt, 3, base, dims, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+  if (enc(halo, dt, 3, base, dims_h, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  if (enc(pw, dt, 3, base, dims, strides, box_p, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+  if (enc(pw, dt, 3, base, dims_p, strides, box_p, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   return true;
 }
