@@ -169,14 +169,18 @@ struct Class {
   std::vector<int> horder;
   std::vector<int> hfirst;
   int nitems = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
+  // RK4 step graphs: without reductions, and with the per-solve norm (the
+  // last step of a chunk)
+  cudaGraph_t graph = nullptr, graph_n = nullptr;
+  cudaGraphExec_t gexec = nullptr, gexec_n = nullptr;
   cudaStream_t st = nullptr;  // classes run concurrently, one stream each
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
-    gexec = nullptr;
-    graph = nullptr;
+    if (gexec_n) cudaGraphExecDestroy(gexec_n);
+    if (graph_n) cudaGraphDestroy(graph_n);
+    gexec = gexec_n = nullptr;
+    graph = graph_n = nullptr;
   }
 };
 
@@ -398,9 +402,35 @@ int ensure_stream(gpe_pool* P, Class& c) {
   return GPE_OK;
 }
 
+// Capture one RK4 step of a class: the queue reset and four batched
+// launches; with_norm: stage 4 reads table row 3 (norm on) and writes the
+// partials, else row 4 (norm off) and no partials.
+int capture_rk4_step(gpe_pool* P, Class& c, int cm, int ns, const int* grids, bool with_norm,
+                     cudaGraph_t* graph, cudaGraphExec_t* gexec) {
+  const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_3, K_RK4_4};
+  PCU(P, cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemsetAsync(c.queue.p, 0, 4 * sizeof(int), c.st);
+  for (int m = 0; m < 4 && e == cudaSuccess; ++m) {
+    const int row = (m == 3 && !with_norm) ? 4 : m;
+    e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)row * ns, c.items.p, c.order.p, c.nitems,
+                     c.queue.p + m, (m == 3 && with_norm) ? c.part.p : nullptr, nullptr);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(c.st, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return pfail(P, GPE_ERR_CUDA, std::string("capturing the batched RK4 step failed: ") +
+                                      cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  *graph = g;
+  PCU(P, cudaGraphInstantiate(gexec, g, 0));
+  return GPE_OK;
+}
+
 // Enqueue `chunk` RK4 steps of every solve of an RK4 class on the class's
-// stream (the step is a captured graph of four batched launches), then the
-// per-solve norm of the result; returns without waiting.
+// stream (each step a captured graph of four batched launches; only the last
+// one forms the per-solve norm of the result), then the norm's finalisation;
+// returns without waiting.
 int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
   Class& c = P->cls[cm][FAM_RK4];
   const int ns = (int)c.solves.size();
@@ -409,36 +439,28 @@ int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
     c.drop_graph();
     PCU(P, cudaStreamSynchronize(c.st));
     if (int rc = build_items(P, c, c.solves)) return rc;
-    PCU(P, c.tab.ensure((size_t)4 * ns));
-    PCU(P, c.htab.ensure((size_t)4 * ns));
+    // table rows: stages 1-4, then stage 4 without the norm
+    PCU(P, c.tab.ensure((size_t)5 * ns));
+    PCU(P, c.htab.ensure((size_t)5 * ns));
     std::vector<BatchStage> t4(4);
     for (int q = 0; q < ns; ++q) {
       rk4_tables(P, c.solves[q], t4.data());
       for (int m = 0; m < 4; ++m) c.htab.p[(size_t)m * ns + q] = t4[m];
+      BatchStage b = t4[3];
+      b.args.want_norm = 0;
+      c.htab.p[(size_t)4 * ns + q] = b;
     }
-    PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)4 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
+    PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)5 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
     const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_3, K_RK4_4};
     int grids[4];
     for (int m = 0; m < 4; ++m) grids[m] = grid_for(cm, kinds[m], c.nitems);
-    // capture one RK4 step of the whole class
     PCU(P, cudaStreamSynchronize(c.st));
-    PCU(P, cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaMemsetAsync(c.queue.p, 0, 4 * sizeof(int), c.st);
-    for (int m = 0; m < 4 && e == cudaSuccess; ++m)
-      e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)m * ns, c.items.p, c.order.p, c.nitems,
-                       c.queue.p + m, m == 3 ? c.part.p : nullptr, nullptr);
-    cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(c.st, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return pfail(P, GPE_ERR_CUDA, std::string("capturing the batched RK4 step failed: ") +
-                                        cudaGetErrorString(e != cudaSuccess ? e : e2));
-    }
-    c.graph = g;
-    PCU(P, cudaGraphInstantiate(&c.gexec, c.graph, 0));
+    if (int rc = capture_rk4_step(P, c, cm, ns, grids, false, &c.graph, &c.gexec)) return rc;
+    if (int rc = capture_rk4_step(P, c, cm, ns, grids, true, &c.graph_n, &c.gexec_n)) return rc;
     c.dirty = false;
   }
-  for (int64_t q = 0; q < chunk; ++q) PCU(P, cudaGraphLaunch(c.gexec, c.st));
+  for (int64_t q = 0; q + 1 < chunk; ++q) PCU(P, cudaGraphLaunch(c.gexec, c.st));
+  if (chunk > 0) PCU(P, cudaGraphLaunch(c.gexec_n, c.st));
   k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
   PCU(P, cudaGetLastError());
   PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));

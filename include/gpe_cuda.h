@@ -70,6 +70,8 @@ typedef struct {
   int32_t storage;         /* GPE_C128 | GPE_C64 device storage of psi/stages */
   int32_t compute;         /* GPE_COMPUTE_* (GPE_C64 storage only)            */
   int32_t tile_zc;         /* z planes per CTA work item; 0 = library default  */
+                           /* (single solve: enough items to fill the GPU;    */
+                           /*  pooled solve: 16 up to nz = 48, else 32)       */
   int32_t reserved;        /* must be 0                                        */
   double xr, yr, zr;       /* half box lengths                                 */
   double tau;              /* |dt| (run.in tau)                                */
