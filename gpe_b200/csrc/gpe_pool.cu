@@ -108,7 +108,6 @@ struct Solve {
   int status = GPE_OK;
   double t_submit = 0, t_start = -1;
   CUtensorMap halo[9], pw[9];
-  int items() const { return ntx * nty * ntz; }
 };
 
 template <class T>

@@ -405,14 +405,18 @@ struct BatchItem {
   int solve, bx, by, bz;
 };
 
-// CTAs per SM the batched RK4 kernels' registers are fitted to.  The R = 1
-// and R = 2 item bodies share one kernel, so unbounded they take 96-128
-// registers at FP32 and 124-154 at FP64; bounded to 6 CTAs of 128 threads
-// (80 registers) at FP32 and 4 (128) at FP64 they spill a few words and run
-// 2-4 % faster on a batch of uneven solves.
+// CTAs per SM the batched kernels' registers are fitted to.  The R = 1 and
+// R = 2 item bodies share one kernel, so unbounded they take 96-128
+// registers (RK4) and 136-185 (Cash-Karp) at FP32, 124-154 and 190-229 at
+// FP64.  Bounded, they spill at most a few words: RK4 to 6 CTAs of 128
+// threads at FP32 (80 registers) and 4 at FP64 (+2-4 % on a batch of uneven
+// solves); Cash-Karp to 4 at FP32 (+8 % on a batch of RKF45 solves) and 3
+// at FP64 (neutral; stages 3-6 are held to 2 CTAs by shared memory anyway).
 template <class C, int KIND>
 __host__ __device__ constexpr int batch_min_blocks() {
-  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) ? (sizeof(C) == 4 ? 6 : 4) : 1;
+  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) ? (sizeof(C) == 4 ? 6 : 4)
+       : (KIND >= K_CK_1 && KIND <= K_CK_6)                                         ? (sizeof(C) == 4 ? 4 : 3)
+                                                                                     : 1;
 }
 
 template <class S, class C, int KIND, int TY, int PY>

@@ -74,6 +74,8 @@ def test_pool_mix_equals_alone_bitwise(gpu):
         out, s = run_alone_handle(rp, state(rp, i), steps)
         np.testing.assert_array_equal(r.psi, out)
         assert r.t == s.t and r.im_t == s.im_t
+        # the pool's norm is that of the final state (formed on a chunk's last step only)
+        assert r.norm == pytest.approx(s.get_norm(), rel=1e-12)
         if rp.scheme == "rk45":
             assert r.dt == s.dt
 
