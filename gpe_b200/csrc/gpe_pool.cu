@@ -166,6 +166,9 @@ struct Class {
   HostPinned<double> hres;
   std::vector<BatchItem> hitems;
   std::vector<int> horder;
+  // the solves (in order) the device work list was built for; an RKF45 class
+  // keeps it across attempts while no solve joins or leaves (dirty stays false)
+  std::vector<Solve*> built_for;
   std::vector<int> hfirst;
   int nitems = 0;
   // RK4 step graphs: without reductions, and with the per-solve norm (the
@@ -350,6 +353,7 @@ void rk45_tables(gpe_pool* P, Solve* s, BatchStage* t6) {
 
 // Work list of the given solves (in order) into the class buffers.
 int build_items(gpe_pool* P, Class& c, const std::vector<Solve*>& sv) {
+  c.built_for = sv;
   c.hitems.clear();
   c.hfirst.assign(1, 0);
   for (Solve* s : sv) {
@@ -494,7 +498,10 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
   if (sv.empty()) return GPE_OK;
   if (int rc = ensure_stream(P, c)) return rc;
   const int ns = (int)sv.size();
-  if (int rc = build_items(P, c, sv)) return rc;
+  if (c.dirty || sv != c.built_for) {
+    if (int rc = build_items(P, c, sv)) return rc;
+    c.dirty = false;
+  }
   PCU(P, c.tab.ensure((size_t)6 * ns));
   PCU(P, c.htab.ensure((size_t)6 * ns));
   std::vector<BatchStage> t6(6);
