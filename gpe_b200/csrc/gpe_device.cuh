@@ -286,6 +286,7 @@ struct Nb {
 // Per-column constants hoisted out of the z loop.
 struct ColumnConsts {
   double wxy, vxy, sxy, rxy2;
+  float vh;  // 0.5 (vx + vy) rounded once, for FP32 compute
   int gx, gy;
 };
 
@@ -293,6 +294,7 @@ __device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i,
   ColumnConsts c;
   c.wxy = active ? a.wx[i] * a.wy[j] : 0.0;
   c.vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
+  c.vh = (float)(0.5 * c.vxy);
   c.sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
   c.rxy2 = (active && a.eqn == 3) ? a.cx[i] * a.cx[i] + a.cy[j] * a.cy[j] : 0.0;
   c.gx = ghost_pos(i, a.g.nx, R, a.bcs);
@@ -313,12 +315,18 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
 #pragma unroll
   for (int q = 0; q < PY; ++q) n2[q] = p[q].r * p[q].r + p[q].i * p[q].i;
   if (a.eqn == 4) {
-    // -(i + gamma) * (-0.5 lap + V psi + g |psi|^2 psi - mu psi)
+    // -(i + gamma) * (-0.5 lap + V psi + g |psi|^2 psi - mu psi).  V in
+    // FP64 as 0.5 ((vx + vy) + vz); in FP32 compute as the sum of the
+    // column's and the plane's halves, each rounded once to float (no FP64
+    // operations or conversions per site)
     const double vz = a.vz[k];
+    const float vzh = (float)(0.5 * vz);
     const C g = (C)a.g_nl, mu = (C)a.mu, gm = (C)a.gamma;
 #pragma unroll
     for (int q = 0; q < PY; ++q) {
-      const C v = (C)(0.5 * (cc[q].vxy + vz));
+      C v;
+      if constexpr (sizeof(C) == sizeof(double)) v = (C)(0.5 * (cc[q].vxy + vz));
+      else v = cc[q].vh + vzh;
       const C wr = ((-(C)0.5 * lap[q].r + v * p[q].r) + g * (n2[q] * p[q].r)) - mu * p[q].r;
       const C wi = ((-(C)0.5 * lap[q].i + v * p[q].i) + g * (n2[q] * p[q].i)) - mu * p[q].i;
       r[q].r = wi - gm * wr;

@@ -224,6 +224,23 @@ def test_fp32_storage_vs_fp64_oracle(gpu, compute):
     assert drift <= 1e-7
 
 
+def test_fp32_storage_trapped_vs_fp64_oracle(gpu):
+    # eqn 4 with a trap: the FP32 stencil forms V from float halves
+    rp = c1_params(nx=40, ny=40, nz=40, xr=9.75, yr=9.75, zr=9.75, bcs=2, order=4, eqn_to_solve=4,
+                   tau=0.005, mu=5.0, omx=0.1, omy=0.1, omz=0.15)
+    psi0 = ic.fermi(rp) * ic.vortex_line_pade(rp, dir="z")
+    o = Oracle(rp)
+    ref = o.run(psi0, 200)
+    s = Solver(rp.replace(storage="c64", compute="f32"))
+    s.set_state(psi0)
+    info = s.solver(200, want_norm=True)
+    err = rel_l2(s.get_state(), ref)
+    drift = abs(info.norm - o.get_norm(ref)) / o.get_norm(ref)
+    print(f"fp32 storage, trapped: rel_l2={err:.3e} norm drift={drift:.3e}")
+    assert err <= 1e-5
+    assert drift <= 1e-7
+
+
 @pytest.mark.slow
 def test_c2_256_cubed_periodic_o4(gpu):
     rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
