@@ -114,15 +114,17 @@ class ServeReport:
 
 
 def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime: bool = True,
-          prep_threads: int = 4, device_ics: bool = True, max_active_sites: int = 160 << 20) -> ServeReport:
+          prep_threads: int = 4, device_ics: bool = True, max_active_sites: int = 160 << 20,
+          on_result=None) -> ServeReport:
     """Run the request stream through one Pool.  With realtime=True a request
     becomes visible at its arrival time on the host clock; every loop turn
     admits what has arrived and fits, advances the batch by up to `chunk`
     steps, and collects finished solves.  device_ics=True builds each
     initial state on the GPU at admission; False prepares it on host
-    threads and copies it in."""
+    threads and copies it in.  on_result(request, result), if given, sees
+    every finished solve before its result buffer is reused."""
     if device_ics:
-        return _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
+        return _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result)
     pool = Pool(budget_bytes)
     rep = ServeReport()
     pending = sorted(requests, key=lambda r: r.arrival_s)
@@ -160,6 +162,8 @@ def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime:
             req = by_tag[r.tag]
             rep.latencies_s[r.tag] = done_t - req.arrival_s
             rep.site_updates += req.sites * r.steps
+            if on_result:
+                on_result(req, r)
     rep.wall_s = time.perf_counter() - t0
     prep.shutdown()
     pool.close()
@@ -191,7 +195,7 @@ def _storage_dtype(params) -> np.dtype:
     return np.dtype(np.complex64 if params.storage == "c64" else np.complex128)
 
 
-def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites) -> ServeReport:
+def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result=None) -> ServeReport:
     """Admission is first-come first-served, bounded by the HBM budget and by
     max_active_sites: enough grid sites in flight to keep the GPU's memory
     system busy, no more, so that early requests are not slowed by every
@@ -238,6 +242,8 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites)
             rep.latencies_s[r.tag] = done_t - req.arrival_s
             rep.site_updates += req.sites * r.steps
             active_sites -= req.sites
+            if on_result:
+                on_result(req, r)
             bufs.put(r.psi)  # the state has been delivered; the buffer serves the next request
     rep.wall_s = time.perf_counter() - t0
     pool.close()
