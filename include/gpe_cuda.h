@@ -24,6 +24,7 @@
 #ifndef GPE_CUDA_H
 #define GPE_CUDA_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
