@@ -26,6 +26,9 @@ GPE_EULER, GPE_RK2, GPE_RK4, GPE_RK45 = 0, 1, 2, 3
 GPE_C128, GPE_C64 = 0, 1
 GPE_COMPUTE_AUTO, GPE_COMPUTE_F32, GPE_COMPUTE_F64 = 0, 1, 2
 
+# planes of built-in scratch in gpe_norm_noalloc (include/gpe_cuda.h)
+GPE_NOALLOC_MAX_NZ = 8192
+
 SCHEMES = {"euler": GPE_EULER, "rk2": GPE_RK2, "rk4": GPE_RK4, "rk45": GPE_RK45}
 
 

@@ -16,8 +16,16 @@
 // it is only a stand-in symbol.  The first call on each device, with that
 // device current, looks up the real device address with
 // cudaGetSymbolAddress and caches it per device; kernels get that pointer.
-// Because this first call also makes the runtime load the module on that
-// device, make it before any stream capture.
+// The same first call loads both dtype instances of the reduction kernel on
+// that device (cudaFuncGetAttributes), so with lazy module loading no later
+// call loads code; make it before any stream capture.  The cached address is
+// not refreshed after cudaDeviceReset or a primary-context reset, which this
+// entry point does not support.
+//
+// Pointers are checked for the alignment the kernels read and write with
+// (16 bytes for complex128 input, 8 for complex64 input and the output
+// double) before anything is launched: a misaligned pointer is rejected
+// with GPE_ERR_BADARG rather than faulting the caller's context.
 //
 // All calls share the one array.  Every call overwrites each partial it
 // reads before reading it, so nothing has to be cleared between calls, but
@@ -26,7 +34,10 @@
 // the caller.
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <cstdint>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/gpe_cuda.h"
 
@@ -35,7 +46,9 @@ namespace {
 static __device__ __align__(256) double g_norm_scratch[GPE_NOALLOC_MAX_NZ];
 
 constexpr int kMaxDevices = 64;
-double* g_scratch_addr[kMaxDevices];  // device address of g_norm_scratch, per device
+// device address of g_norm_scratch, per device; written once under g_setup
+std::atomic<double*> g_scratch_addr[kMaxDevices];
+std::mutex g_setup;
 
 // Extended closed (Numerical Recipes 4.1.14) weights of integrate_x/y/z
 // (src/variables.f90:49-51, 730-840): 3/8, 7/6, 23/24 at both ends, 1 inside.
@@ -94,6 +107,26 @@ int reject(const char* why) {
   return GPE_ERR_BADARG;
 }
 
+// Set-up of the current device (once): the scratch array's device address,
+// and both reduction kernels loaded.  Returns nullptr on a CUDA error.
+double* scratch_of(int dev) {
+  double* p = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (p) return p;
+  std::lock_guard<std::mutex> lk(g_setup);
+  p = g_scratch_addr[dev].load(std::memory_order_relaxed);
+  if (p) return p;
+  void* addr = nullptr;
+  if (cudaGetSymbolAddress(&addr, g_norm_scratch) != cudaSuccess || !addr) return nullptr;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_plane_sums<double2>) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k_plane_sums<float2>) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k_plane_total) != cudaSuccess)
+    return nullptr;
+  p = (double*)addr;
+  g_scratch_addr[dev].store(p, std::memory_order_release);
+  return p;
+}
+
 }  // namespace
 
 extern "C" int gpe_norm_noalloc(const void* psi_dev, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, double dx,
@@ -102,14 +135,15 @@ extern "C" int gpe_norm_noalloc(const void* psi_dev, int32_t dtype, int32_t nx, 
   if (dtype != GPE_C128 && dtype != GPE_C64) return reject("dtype must be GPE_C128 or GPE_C64");
   if (nx < 6 || ny < 6 || nz < 6) return reject("nx, ny and nz must be >= 6");
   if (nz > GPE_NOALLOC_MAX_NZ) return reject("nz exceeds GPE_NOALLOC_MAX_NZ (8192 planes of scratch)");
+  const uintptr_t in_align = dtype == GPE_C128 ? 16 : 8;
+  if ((uintptr_t)psi_dev % in_align != 0)
+    return reject(dtype == GPE_C128 ? "psi_dev is not 16-byte aligned (complex128)"
+                                    : "psi_dev is not 8-byte aligned (complex64)");
+  if ((uintptr_t)norm_dev % 8 != 0) return reject("norm_dev is not 8-byte aligned");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GPE_ERR_CUDA;
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_norm_scratch) != cudaSuccess || !p) return GPE_ERR_CUDA;
-    g_scratch_addr[dev] = (double*)p;
-  }
-  double* scratch = g_scratch_addr[dev];
+  double* scratch = scratch_of(dev);
+  if (!scratch) return GPE_ERR_CUDA;
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == GPE_C128)
     k_plane_sums<double2><<<nz, 256, 0, st>>>((const double2*)psi_dev, nx, ny, scratch);

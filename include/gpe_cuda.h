@@ -379,10 +379,13 @@ int64_t gpe_state_bytes(const gpe_params* p);
  * (GPE_NOALLOC_MAX_NZ doubles, 64 KiB), resident on every GPU that loads the
  * library until the process exits.  nz > GPE_NOALLOC_MAX_NZ (or nx, ny,
  * nz < 6, a bad dtype, a NULL pointer) returns GPE_ERR_BADARG and prints the
- * reason on stderr.  The first call on a device looks up the array's device
- * address (and so loads the module there); make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller.
+ * reason on stderr, and so does a psi_dev that is not aligned to its element
+ * (16 bytes for complex128, 8 for complex64) or a norm_dev that is not
+ * 8-byte aligned; nothing is launched then.  The first call on a device
+ * looks up the array's device address and loads the kernels of both dtypes
+ * there; make it before any stream capture.  A device reset after that
+ * first call is not supported.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.
  */
 #define GPE_NOALLOC_MAX_NZ 8192
 int gpe_norm_noalloc(const void* psi_dev, int32_t dtype, int32_t nx, int32_t ny, int32_t nz, double dx, double dy,

@@ -85,3 +85,23 @@ def test_no_cpu_fallback_without_gpu():
     rc = lib.gpe_create(C.byref(p), C.byref(h))
     assert rc == L.GPE_ERR_CUDA
     assert not h.value
+
+
+def test_norm_noalloc_rejects_misaligned_pointers_before_any_launch():
+    """gpe_norm_noalloc checks its caller-owned pointers for the alignment its
+    kernels load and store with, and returns GPE_ERR_BADARG without touching
+    the device (these addresses are never dereferenced: the call is rejected
+    before any CUDA call, which also holds without a GPU)."""
+    lib = L.load()
+    args = (6, 6, 6, 1.0, 1.0, 1.0)
+    good = 0x10000
+    # complex128 input must be 16-byte aligned
+    assert lib.gpe_norm_noalloc(C.c_void_p(good + 8), L.GPE_C128, *args, C.c_void_p(good), None) == L.GPE_ERR_BADARG
+    # complex64 input 8-byte aligned
+    assert lib.gpe_norm_noalloc(C.c_void_p(good + 4), L.GPE_C64, *args, C.c_void_p(good), None) == L.GPE_ERR_BADARG
+    # the output double 8-byte aligned
+    assert lib.gpe_norm_noalloc(C.c_void_p(good), L.GPE_C64, *args, C.c_void_p(good + 4), None) == L.GPE_ERR_BADARG
+    # size limit and dtype, also before any CUDA call
+    assert lib.gpe_norm_noalloc(C.c_void_p(good), L.GPE_C128, 6, 6, L.GPE_NOALLOC_MAX_NZ + 1, 1.0, 1.0, 1.0,
+                                C.c_void_p(good), None) == L.GPE_ERR_BADARG
+    assert lib.gpe_norm_noalloc(C.c_void_p(good), 7, *args, C.c_void_p(good), None) == L.GPE_ERR_BADARG
