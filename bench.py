@@ -242,6 +242,44 @@ def fp32_storage_leg(args, torch, psi0):
     return out
 
 
+ACC_STEPS = 2000
+
+
+def fp32_accuracy_leg(psi0, steps: int = ACC_STEPS):
+    """Accuracy of complex64 storage at the full workload: the 256^3 random
+    phase state advanced `steps` RK4 steps (dt = 0.005) with complex64
+    storage, against the complex128 FP64 GPU path from the same initial
+    state (that path matches the FP64 CPU oracle to <= 1e-12 relative L2 in
+    the parity tests).  rel_l2 = |psi32 - psi64| / |psi64| over all sites;
+    norm / energy drift = |X32 - X64| / |X64| at the final step (get_norm
+    quadrature; energy() as the reference defines it)."""
+    from gpe_b200.solver import RunParams, Solver
+
+    def run(**kw):
+        s = Solver(RunParams(**WORKLOAD, **kw))
+        s.set_state(psi0)
+        n0, e0 = s.get_norm(), s.energy()
+        s.solver(steps)
+        out = s.get_state()
+        n1, e1 = s.get_norm(), s.energy()
+        s.close()
+        return out, n0, e0, n1, e1
+
+    ref, n0, e0, nref, eref = run()
+    den = float(np.linalg.norm(ref.ravel()))
+    res = {"steps": steps, "reference": "complex128 FP64 GPU path from the same initial state (parity tests pin it "
+                                        "to the FP64 CPU oracle at <= 1e-12 rel L2)",
+           "fp64_self_norm_drift": abs(nref - n0) / n0, "fp64_self_energy_drift": abs(eref - e0) / abs(e0)}
+    for compute in ("f32", "f64"):
+        out, _, _, n1, e1 = run(storage="c64", compute=compute)
+        res[compute + "_compute"] = {
+            "rel_l2": float(np.linalg.norm((out - ref).ravel())) / den,
+            "norm_drift": abs(n1 - nref) / nref,
+            "energy_drift": abs(e1 - eref) / abs(eref)}
+        del out
+    return res
+
+
 def rk45_leg(args, torch):
     """Trapped-condensate RKF45 workload: 192x192x384, dx = 0.25, reflective,
     4th order, eqn 4 with damping gamma = 0.05, mu = 10, trap (0.05, 0.05,
@@ -556,9 +594,10 @@ def main() -> int:
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
             "e2e": e2e, "roofline": roofline, "clocks": clk.summary(), "gpu_launches": gpu_launches}
-    if not args.no_extras:
+    if not args.no_extras and ws == 1:  # the extra legs are single-GPU workloads
         line["fp32_storage"] = fp32_storage_leg(args, torch, psi0)
         line["fp32_storage"]["speedup_vs_fp64"] = line["fp32_storage"]["f32_compute"]["value"] / (value / ws)
+        line["fp32_storage"]["accuracy"] = fp32_accuracy_leg(psi0)
         line["rk45_trapped"] = rk45_leg(args, torch)
         line["batched_c4"] = batched_leg(args, torch)
         line["batched_c4"]["speedup_vs_plain_fp64"] = line["batched_c4"]["value"] / (value / ws)

@@ -144,6 +144,8 @@ _PROTOS = {
     "gpe_pool_solve_bytes": (C.c_int64, [C.POINTER(GpeParams)]),
     "gpe_pool_last_error": (C.c_char_p, [C.c_void_p]),
     "gpe_pool_destroy": (None, [C.c_void_p]),
+    "gpe_test_expire_waits": (C.c_int, [C.c_void_p]),
+    "gpe_pool_test_expire_waits": (C.c_int, [C.c_void_p]),
     "gpe_norm_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_double,
                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
 }

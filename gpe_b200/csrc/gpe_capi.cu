@@ -1060,6 +1060,14 @@ int gpe_sync(gpe_handle* h) {
   return check_status(h);
 }
 
+int gpe_test_expire_waits(gpe_handle* h) {
+  if (!h) return GPE_ERR_BADARG;
+  CU(h, cudaSetDevice(h->dev));
+  static const int v = STATUS_EXPIRE_TEST;
+  CU(h, cudaMemcpyAsync(h->status, &v, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  return GPE_OK;
+}
+
 int gpe_profile(gpe_handle* h, int32_t enable) {
   if (!h) return GPE_ERR_BADARG;
   CU(h, cudaSetDevice(h->dev));

@@ -164,6 +164,7 @@ struct Class {
   DevBuf<double> res;       // [solve][RED_SLOTS]
   HostPinned<BatchStage> htab;
   HostPinned<double> hres;
+  HostPinned<int> hstatus;  // device status word after the class's last RKF45 attempt
   std::vector<BatchItem> hitems;
   std::vector<int> horder;
   // the solves (in order) the device work list was built for; an RKF45 class
@@ -517,6 +518,10 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
   k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
   PCU(P, cudaGetLastError());
   PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  // the status word comes back with the error norms: an attempt whose
+  // bounded waits expired has no usable error norm to act on
+  PCU(P, c.hstatus.ensure(1));
+  PCU(P, cudaMemcpyAsync(c.hstatus.p, P->d_status, sizeof(int), cudaMemcpyDeviceToHost, c.st));
   return GPE_OK;
 }
 
@@ -524,6 +529,12 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
 int rk45_collect(gpe_pool* P, int cm, const std::vector<Solve*>& sv) {
   Class& c = P->cls[cm][FAM_RK45];
   PCU(P, cudaStreamSynchronize(c.st));
+  if (c.hstatus.p[0] != 0) {
+    // the attempt did not complete: these solves stop here (retired with
+    // GPE_ERR_TIMEOUT by gpe_pool_step)
+    for (Solve* s : sv) s->status = GPE_ERR_TIMEOUT;
+    return GPE_OK;
+  }
   for (size_t q = 0; q < sv.size(); ++q) {
     Solve* s = sv[q];
     const gpe_params& p = s->p;
@@ -748,7 +759,17 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
   for (int cm = 0; cm < NCM; ++cm)
     if (chunks[cm])
       if (int rc = rk4_collect(P, cm, chunks[cm])) return rc;
-  if (int rc = check_status(P)) return rc;
+  // a stage kernel whose bounded waits expired left the status word set: the
+  // solves of this step have states that cannot be trusted, so they are
+  // retired with GPE_ERR_TIMEOUT (their results say so) and the call reports
+  // the error; the pool itself stays usable
+  const int timeout_rc = check_status(P);
+  if (timeout_rc == GPE_ERR_TIMEOUT)
+    for (int cm = 0; cm < NCM; ++cm)
+      for (int fam = 0; fam < NFAM; ++fam)
+        for (Solve* s : P->cls[cm][fam].solves) s->status = GPE_ERR_TIMEOUT;
+  else if (timeout_rc)
+    return timeout_rc;
   // retire finished solves
   int active = 0;
   for (int cm = 0; cm < NCM; ++cm)
@@ -792,6 +813,15 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
       active += (int)c.solves.size();
     }
   if (n_active) *n_active = active;
+  return timeout_rc;
+}
+
+int gpe_pool_test_expire_waits(gpe_pool* P) {
+  if (!P) return GPE_ERR_BADARG;
+  PCU(P, cudaSetDevice(P->dev));
+  PCU(P, cudaDeviceSynchronize());
+  const int v = STATUS_EXPIRE_TEST;
+  PCU(P, cudaMemcpy(P->d_status, &v, sizeof(int), cudaMemcpyHostToDevice));
   return GPE_OK;
 }
 
@@ -846,6 +876,7 @@ void gpe_pool_destroy(gpe_pool* P) {
       c.res.free();
       c.htab.free();
       c.hres.free();
+      c.hstatus.free();
     }
   if (P->arena) cudaFree(P->arena);
   if (P->d_status) cudaFree(P->d_status);

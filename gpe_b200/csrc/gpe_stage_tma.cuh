@@ -65,17 +65,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: gives up after ~2^31 SM cycles (about a second) or 2^26
-// polls, whichever comes first.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Bounded wait: gives up after ~2^31 SM cycles (about a second) or
+// max_polls polls, whichever comes first.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int max_polls = 1 << 26) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  for (int it = 0; it < (1 << 26); ++it) {
+  for (int it = 0; it < max_polls; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (clock64() - t0 > (1LL << 31)) break;
   }
   return false;
 }
+
+// Device status word values (StageArgs::status).  STATUS_EXPIRE_TEST is set
+// by the host only (gpe_test_expire_waits): while it stands, every work item
+// first waits, with a short limit, on a barrier that nothing arrives at, so
+// that the timeout path (abort, drain the issued copies, return) runs; the
+// word keeps the value until the host reads and clears it.
+constexpr int STATUS_OK = 0;
+constexpr int STATUS_WAIT_EXPIRED = 1;
+constexpr int STATUS_EXPIRE_TEST = 2;
+constexpr int EXPIRE_TEST_POLLS = 1 << 10;
 
 // Copy stage arguments from the device table through the read-only path.
 __device__ __forceinline__ StageArgs __ldg_args(const StageArgs* p) {
@@ -118,9 +128,11 @@ template <class S, int RMAX, int NPW, int TY>
 struct TmaLayout {
   static constexpr int NSS = 2 * RMAX + 2;  // stencil ring slots
   static constexpr int NPS = 3;             // point-wise ring slots
+  static constexpr int NEVER_BAR = 15;      // barrier nothing arrives at (timeout test), last of 16
   static constexpr uint32_t ST_SLOT = round128(tma_st_bytes<S>(RMAX, TY));
   static constexpr uint32_t PW_SLOT = round128(NPW * tma_pw1_bytes<S>(TY));
   static constexpr uint32_t BAR_BYTES = 128;
+  static_assert(NSS + NPS <= NEVER_BAR, "ring barriers overlap the never-arriving one");
   // dynamic shared memory: barriers + rings + 128 B of alignment slack
   static constexpr uint32_t SMEM = BAR_BYTES + NSS * ST_SLOT + (NPW > 0 ? NPS * PW_SLOT : 0) + 128;
 };
@@ -131,6 +143,7 @@ struct TmaLayout {
 struct TmaRing {
   uint64_t* sbar;
   uint64_t* pbar;
+  uint64_t* nbar;  // no thread or copy ever arrives here
   unsigned char* sring;
   unsigned char* pring;
   int sbase, pbase;  // loads issued for earlier work items
@@ -145,6 +158,7 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
   TmaRing rg;
   rg.sbar = (uint64_t*)smem;
   rg.pbar = rg.sbar + LY::NSS;
+  rg.nbar = rg.sbar + LY::NEVER_BAR;
   rg.sring = smem + LY::BAR_BYTES;
   rg.pring = rg.sring + LY::NSS * LY::ST_SLOT;
   rg.sbase = rg.pbase = 0;
@@ -152,6 +166,7 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
     *s_abort = 0;
     for (int s = 0; s < LY::NSS; ++s) mbar_init(&rg.sbar[s], 1);
     for (int s = 0; s < LY::NPS; ++s) mbar_init(&rg.pbar[s], 1);
+    mbar_init(rg.nbar, 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -212,7 +227,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   // (bounded), then leave
   auto drain = [&](int waited_s, int waited_p) {
     if (tid == 0) {
-      atomicExch(a.status, 1);
+      atomicCAS(a.status, STATUS_OK, STATUS_WAIT_EXPIRED);  // a standing test value stays
       for (int l = waited_s; l < issued_s; ++l) swait(l);
       for (int m = waited_p; m < issued_p; ++m) pwait(m);
     }
@@ -246,6 +261,11 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
   S q[PY][2 * R + 1];  // z queue of each owned row: planes k-R .. k+R
   bool ok = true;
+  // timeout test (host-armed only): wait, with a short limit, on the barrier
+  // nothing arrives at; it expires and the item takes the abort path below
+  // with its first copies in flight
+  if (*(volatile const int*)a.status == STATUS_EXPIRE_TEST)
+    ok = mbar_wait_bounded(rg.nbar, 0, EXPIRE_TEST_POLLS);
 #pragma unroll
   for (int l = 0; l < 2 * R; ++l) {
     ok &= swait(l);

@@ -309,6 +309,17 @@ int gpe_profile(gpe_handle* h, int32_t enable);
  * each input field, one write of each output field). */
 int gpe_profile_get(gpe_handle* h, int32_t kind, double* total_ms, int64_t* launches, double* bytes_per_site);
 
+/* Testing aid for the timeout path (the reference's counterpart is the
+ * emergency_stop convention of src/error.f90:24-46 that a host applies to
+ * GPE_ERR_TIMEOUT).  Arms the handle's device status word so that every
+ * stage-kernel work item queued after this call first waits, with a short
+ * limit, on a shared-memory barrier that nothing arrives at: the wait
+ * expires, the CTA lets the copies it has issued land (bounded wait) and
+ * returns without storing anything.  The next gpe_step / gpe_sync that reads
+ * the word returns GPE_ERR_TIMEOUT and clears it; the handle stays usable.
+ * After any GPE_ERR_TIMEOUT the state is unspecified: set it again. */
+int gpe_test_expire_waits(gpe_handle* h);
+
 /*
  * Batched solves and serving (no reference counterpart: the reference runs
  * exactly one solve per MPI job).  A pool owns one device arena of
@@ -348,6 +359,11 @@ int64_t gpe_pool_free_bytes(const gpe_pool* pool);
 /* Arena bytes one solve with these parameters needs (state + tables). */
 int64_t gpe_pool_solve_bytes(const gpe_params* p);
 const char* gpe_pool_last_error(const gpe_pool* pool);
+/* The pool's form of gpe_test_expire_waits: the next gpe_pool_step returns
+ * GPE_ERR_TIMEOUT, and the solves it was advancing are retired with status
+ * GPE_ERR_TIMEOUT in their results (what a genuine expiry does too); solves
+ * submitted afterwards run normally. */
+int gpe_pool_test_expire_waits(gpe_pool* pool);
 
 /* Page-locked host memory (cudaMallocHost) for the psi0 / out buffers of
  * gpe_pool_submit and the host arrays of gpe_set_state / gpe_get_state:

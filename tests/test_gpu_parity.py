@@ -242,6 +242,71 @@ def test_fp32_storage_trapped_vs_fp64_oracle(gpu):
 
 
 @pytest.mark.slow
+def test_fp32_storage_c2_256_cubed_vs_oracle(gpu):
+    """The roofline workload (256^3 random phase, periodic, 4th order, RK4
+    dt = 0.005, eqn 2) in complex64 storage with the FP32 stencil, 200 steps,
+    against the FP64 CPU oracle on the same initial state."""
+    rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
+                   eqn_to_solve=2, bcs=1, order=4)
+    psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
+    s = Solver(rp.replace(storage="c64", compute="f32"))
+    s.set_state(psi0)
+    s.solver(200)
+    out = s.get_state()
+    n32, e32 = s.get_norm(), s.energy()
+    s.close()
+    o = Oracle(rp)
+    ref = o.run(psi0, 200)
+    nref, eref = o.get_norm(ref), o.energy(ref)
+    err = rel_l2(out, ref)
+    drift = abs(n32 - nref) / nref
+    edrift = abs(e32 - eref) / abs(eref)
+    print(f"fp32 storage 256^3, 200 steps: rel_l2={err:.3e} norm drift={drift:.3e} energy drift={edrift:.3e}")
+    assert err <= 1e-5
+    assert drift <= 1e-7
+
+
+def test_fp32_storage_rk45_trapped_vs_fp64_oracle(gpu):
+    """The trapped RKF45 workload on a smaller grid (48 x 48 x 96, dx = 0.25,
+    reflective, 4th order, eqn 4 with gamma = 0.05, mu = 10, trap (0.05,
+    0.05, 0.025), TF x Pade vortex line, eps = 1e-6): complex64 storage with
+    FP64 step control, 200 accepted steps, against the FP64 oracle's RKF45.
+    The two runs choose their own step sizes, so they end at slightly
+    different times; the oracle is advanced to the FP32 run's final time
+    (its last RKF45 step that stays below it, then one FP64 RK4 step of the
+    remaining interval) and compared there."""
+    rp = RunParams(nx=48, ny=48, nz=96, xr=5.875, yr=5.875, zr=11.875, tau=0.01, scheme="rk45",
+                   eqn_to_solve=4, bcs=2, order=4, g=1.0, mu=10.0, omx=0.05, omy=0.05, omz=0.025, gamma=0.05)
+    psi0 = ic.fermi(rp) * ic.vortex_line_pade(rp, dir="z")
+    s = Solver(rp.replace(storage="c64", compute="f32"))
+    s.set_state(psi0)
+    info = s.solver(200)
+    out = s.get_state()
+    t32, acc32, rej32 = s.t, 200, info.rejected
+    n32 = s.get_norm()
+    s.close()
+    o = Oracle(rp)
+    psi, acc64 = psi0, 0
+    while True:
+        t_before = o.clock.t
+        nxt = o.run(psi, 1)
+        if o.clock.t > t32:
+            break
+        psi, acc64 = nxt, acc64 + 1
+    gap = t32 - t_before
+    assert 0.0 <= gap < 0.05
+    ref = Oracle(rp.replace(scheme="rk4", tau=gap)).run(psi, 1) if gap > 0 else psi
+    nref = o.get_norm(ref)
+    err = rel_l2(out, ref)
+    drift = abs(n32 - nref) / nref
+    print(f"fp32 storage RKF45 trapped: rel_l2={err:.3e} norm drift={drift:.3e} t={t32:.6f} "
+          f"accepted/rejected fp32 {acc32}/{rej32}, fp64 oracle {acc64}/{o.clock.rejected} (to t={t_before:.6f})")
+    assert abs(acc64 - acc32) <= 2
+    assert err <= 1e-5
+    assert drift <= 1e-7
+
+
+@pytest.mark.slow
 def test_c2_256_cubed_periodic_o4(gpu):
     rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
                    eqn_to_solve=2, bcs=1, order=4)
