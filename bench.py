@@ -414,6 +414,34 @@ def ncu_batch_case(args) -> int:
     return 0
 
 
+SERVING_SEED = 2024
+
+
+def serving_leg(n_requests: int, torch):
+    """The serving workload's first n_requests requests (Poisson 20/s, seed
+    2024; sizes 48^3..256^3; 200-5000 RK4/RKF45 steps; order 2/4; V = 0 or a
+    trap; ring / line / random-phase initial states built on the device;
+    FP64 or FP32 storage): continuous batching with shortest-job-first
+    admission from one HBM budget, against the plain one-solve-at-a-time FP64
+    path on the same requests.  Latency = completion - arrival (host clock)."""
+    from gpe_b200 import serve
+
+    reqs = serve.make_requests(n_requests, seed=SERVING_SEED)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free * 0.85)
+    batched = serve.serve(reqs, budget, chunk=50).summary()
+    single = serve.serve_one_at_a_time(reqs).summary()
+    work = sum(r.sites * r.nsteps for r in reqs)
+    return {"requests": len(reqs), "seed": SERVING_SEED, "rate_per_s": 20.0,
+            "offered_site_steps": work, "arrival_span_s": reqs[-1].arrival_s,
+            "offered_site_steps_per_s": work / reqs[-1].arrival_s,
+            "sustained_site_steps_per_s": batched["site_updates_per_s"],
+            "policy": "shortest job first among arrived requests, <= 48 Mi sites in flight, HBM budget 85% of free",
+            "continuous_batching": batched, "one_at_a_time_fp64": single,
+            "throughput_ratio": batched["site_updates_per_s"] / single["site_updates_per_s"],
+            "p50_ratio": batched["p50_s"] / single["p50_s"], "p99_ratio": batched["p99_s"] / single["p99_s"]}
+
+
 def run_serving(args) -> int:
     """Serving sample: the first `--requests` requests of the synthetic
     stream (Poisson 20/s; sizes 48^3..256^3; 200-5000 RK4/RKF45 steps;
@@ -454,6 +482,8 @@ def main() -> int:
     ap.add_argument("--serving", action="store_true",
                     help="serving workload: Poisson stream of mixed solves, continuous batching vs one at a time")
     ap.add_argument("--requests", type=int, default=40, help="--serving: requests in the sample")
+    ap.add_argument("--serving-requests", type=int, default=200,
+                    help="requests of the serving sample on the main line (0 = skip)")
     ap.add_argument("--storage", default="c128", choices=["c128", "c64"],
                     help="storage of the --ncu-case / --quick workload")
     ap.add_argument("--batch", action="store_true",
@@ -598,6 +628,8 @@ def main() -> int:
         line["fp32_storage"] = fp32_storage_leg(args, torch, psi0)
         line["fp32_storage"]["speedup_vs_fp64"] = line["fp32_storage"]["f32_compute"]["value"] / (value / ws)
         line["fp32_storage"]["accuracy"] = fp32_accuracy_leg(psi0)
+        if args.serving_requests > 0:
+            line["serving"] = serving_leg(args.serving_requests, torch)
         line["rk45_trapped"] = rk45_leg(args, torch)
         line["batched_c4"] = batched_leg(args, torch)
         line["batched_c4"]["speedup_vs_plain_fp64"] = line["batched_c4"]["value"] / (value / ws)

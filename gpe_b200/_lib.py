@@ -119,6 +119,7 @@ _PROTOS = {
     "gpe_pool_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeParams), C.POINTER(GpeIC), C.c_int64, C.c_uint64,
                                      C.c_void_p]),
     "gpe_set_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeIC)]),
+    "gpe_multiply_ic": (C.c_int, [C.c_void_p, C.POINTER(GpeIC), C.c_int32]),
     "gpe_condensed": (C.c_int, [C.c_void_p, C.POINTER(GpeCondensedInfo), C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_int32]),
     "gpe_filtered": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_int32]),

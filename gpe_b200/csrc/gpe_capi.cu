@@ -84,7 +84,7 @@ struct gpe_handle {
   long long prof_n[K_NUM] = {0};
   // kernel variant: true = TMA plane pipeline (k_stage_tma), false = k_stage
   bool use_tma = true;
-  int tma_ty = 4;  // threads per CTA in y for the 32 x 8 tile: 4 = two rows per thread, 8 = one
+  int tma_ty = TILE_32x8_ROW2;  // thread layout of the TMA stage kernel (TileVariant)
   std::vector<CUtensorMap> map_halo, map_pw;  // per field
   int* status = nullptr;                      // device status word
   // FFT diagnostics: transform scratch + the reference's k-grid symbols
@@ -157,9 +157,9 @@ int fail(gpe_handle* h, int code, const std::string& msg) {
 int validate(const gpe_params* p, std::string& why) { return validate_params(p, why); }
 void layout(const gpe_params* p, Geom& g, int& esz) { param_layout(p, g, esz); }
 int nfields(int scheme) { return scheme_fields(scheme); }
-int choose_zc(const Geom& g) { return default_zc(g); }
+int choose_zc(const Geom& g, int tile_h) { return default_zc(g, tile_h); }
 bool encode_field_maps(gpe_handle* h, void* base, CUtensorMap* halo, CUtensorMap* pw) {
-  return encode_maps(base, h->g, h->esz, h->R, halo, pw);
+  return encode_maps(base, h->g, h->esz, h->R, halo, pw, tile_rows(h->tma_ty));
 }
 
 int field_of(const gpe_handle* h, const void* p) {
@@ -675,8 +675,19 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
   h->R = p->order / 2;
   h->cmode = p->storage == GPE_C128 ? CM_F64 : (p->compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32);
   h->nelem = padded_elems(h->g);
-  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g);
-  h->grid = dim3((pl.nx + 31) / 32, (pl.ny + 7) / 8, (pl.nz + h->zc - 1) / h->zc);
+  // thread layout: complex64 storage with the FP32 stencil takes two
+  // x-adjacent sites per thread (16-byte shared-memory reads and stores)
+  if (const char* e = getenv("GPE_KERNEL")) h->use_tma = strcmp(e, "ldg") != 0;
+  if (h->cmode == CM_F32 && h->use_tma) h->tma_ty = TILE_PAIR_32x16;
+  if (const char* e = getenv("GPE_ROWS_PER_THREAD")) h->tma_ty = atoi(e) == 1 ? TILE_32x8_ROW1 : TILE_32x8_ROW2;
+  if (const char* e = getenv("GPE_TILE")) {
+    const int v = atoi(e);
+    if (v == TILE_32x8_ROW1 || v == TILE_32x8_ROW2 || (h->cmode == CM_F32 && h->use_tma && tile_is_pair(v)))
+      h->tma_ty = v;
+  }
+  const int th = tile_rows(h->tma_ty);
+  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g, th);
+  h->grid = dim3((pl.nx + 31) / 32, (pl.ny + th - 1) / th, (pl.nz + h->zc - 1) / h->zc);
   h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
   auto bail = [&](int rc) {
     std::string m = h->err;
@@ -701,8 +712,6 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
     }
     cudaMemsetAsync(h->fields[f], 0, (size_t)h->nelem * h->esz, h->st);
   }
-  if (const char* e = getenv("GPE_KERNEL")) h->use_tma = strcmp(e, "ldg") != 0;
-  if (const char* e = getenv("GPE_ROWS_PER_THREAD")) h->tma_ty = atoi(e) == 1 ? 8 : 4;
   if (h->use_tma) {
     h->map_halo.resize(nf);
     h->map_pw.resize(nf);
@@ -1214,6 +1223,19 @@ int gpe_set_ic(gpe_handle* h, const gpe_ic* ic) {
   if (wb)
     if (int rc = ensure_staging(h, wb)) return rc;
   CU(h, ic_generate(h->p, h->g, h->esz, h->R, *ic, h->fields[h->cur], h->staging, h->staging_bytes, h->st));
+  CU(h, cudaStreamSynchronize(h->st));
+  return GPE_OK;
+}
+
+int gpe_multiply_ic(gpe_handle* h, const gpe_ic* ic, int32_t modulus) {
+  if (!h) return GPE_ERR_BADARG;
+  if (h->slab) return fail(h, GPE_ERR_BADARG, "gpe_multiply_ic: not available on a z-slab handle");
+  std::string why;
+  if (int rc = ic_validate(ic, why)) return fail(h, rc, why);
+  if (ic_needs_fft(ic))
+    return fail(h, GPE_ERR_BADARG, "gpe_multiply_ic: the random-phase state cannot multiply a state");
+  CU(h, cudaSetDevice(h->dev));
+  CU(h, ic_multiply(h->p, h->g, h->esz, h->R, *ic, h->fields[h->cur], modulus != 0, h->st));
   CU(h, cudaStreamSynchronize(h->st));
   return GPE_OK;
 }

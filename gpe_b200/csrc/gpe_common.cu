@@ -57,7 +57,7 @@ int scheme_fields(int scheme) {
 }
 
 // z planes per block: enough blocks for several waves on 148 SMs
-int default_zc(const Geom& g) {
+int default_zc(const Geom& g, int tile_h) {
   if (const char* e = getenv("GPE_ZC")) {
     int v = atoi(e);
     if (v > 0) return std::min(v, g.nz);
@@ -65,7 +65,7 @@ int default_zc(const Geom& g) {
   // at most 20 planes per CTA: at 256^3 the sweep 8..32 gives 20 the best
   // rate (FP32 +1.4-1.8 %, FP64 +0.8 % over 16); small grids use fewer so
   // that every SM gets several CTAs.
-  const long long bxy = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+  const long long bxy = (long long)((g.nx + 31) / 32) * ((g.ny + tile_h - 1) / tile_h);
   const long long target = 148LL * 8;
   long long zc = (g.nz * bxy + target - 1) / target;
   zc = std::max<long long>(4, std::min<long long>(zc, 20));
@@ -93,7 +93,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // TMA unit zero-fills the rest of a partial tile instead of reading the
 // row padding from HBM (only lanes outside the grid see those zeros).  No
 // L2 sector promotion: a box row is fetched as the sectors it covers.
-bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw) {
+bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw, int tile_h) {
   auto enc = tensor_map_encoder();
   if (!enc) return false;
   const CUtensorMapDataType dt = esz == 16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -101,8 +101,8 @@ bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, C
   const cuuint64_t dims_p[3] = {(cuuint64_t)(2 * (g.xoff + g.nx)), (cuuint64_t)(g.ny + 4), (cuuint64_t)(g.nz + 4)};
   const cuuint64_t strides[2] = {(cuuint64_t)(g.px * esz), (cuuint64_t)(g.pz * esz)};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const cuuint32_t box_h[3] = {(cuuint32_t)(2 * tma_stencil_w()), (cuuint32_t)tma_stencil_h(8, R), 1};
-  const cuuint32_t box_p[3] = {(cuuint32_t)(2 * TMA_TX), 8, 1};
+  const cuuint32_t box_h[3] = {(cuuint32_t)(2 * tma_stencil_w()), (cuuint32_t)tma_stencil_h(tile_h, R), 1};
+  const cuuint32_t box_p[3] = {(cuuint32_t)(2 * TMA_TX), (cuuint32_t)tile_h, 1};
   if (enc(halo, dt, 3, base, dims_h, strides, box_h, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;

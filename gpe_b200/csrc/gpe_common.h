@@ -23,9 +23,10 @@ long long padded_elems(const Geom& g);
 // fields a scheme keeps per solve
 int scheme_fields(int scheme);
 // z planes per CTA / work item
-int default_zc(const Geom& g);
-// tensor maps of one field: halo'd stencil box and point-wise box (TY = 8)
-bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw);
+int default_zc(const Geom& g, int tile_h = 8);
+// tensor maps of one field: halo'd stencil box and point-wise box of a
+// 32 x tile_h tile
+bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw, int tile_h = 8);
 // algorithmic field elements moved per site by one launch of a stage kind
 int kind_elems(int kind);
 // per-axis tables [vx|vy|vz, sx|sy|sz, wx|wy|wz, x|y|z] and grid spacings

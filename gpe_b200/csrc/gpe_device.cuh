@@ -42,6 +42,19 @@ enum StageKind : int {
   K_NUM
 };
 
+// Thread layouts of the single-solve TMA stage kernel over a 32-column tile.
+// The values of the first two are the kernels' threads in y (the tile is
+// 32 x 8 either way); the pair layouts give every thread two x-adjacent
+// sites (complex64 storage only).
+enum TileVariant : int {
+  TILE_32x8_ROW1 = 8,    // 32 x 8 threads, one site per plane each
+  TILE_32x8_ROW2 = 4,    // 32 x 4 threads, two rows each
+  TILE_PAIR_32x8 = 16,   // 16 x 8 threads, one x pair each
+  TILE_PAIR_32x16 = 32,  // 16 x 8 threads on a 32 x 16 tile, an x pair in two rows each
+};
+__host__ __device__ constexpr int tile_rows(int v) { return v == TILE_PAIR_32x16 ? 16 : 8; }
+__host__ __device__ constexpr bool tile_is_pair(int v) { return v == TILE_PAIR_32x8 || v == TILE_PAIR_32x16; }
+
 // reduction slots in the per-block partials: [norm, energy, errmax]
 enum { RED_NORM = 0, RED_ENERGY = 1, RED_ERR = 2, RED_SLOTS = 3 };
 
@@ -393,11 +406,16 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
 // offset of (i, j_q, k); gz = ghost_pos(k, nz, R, bcs).  Sites with
 // act[q] false (outside the grid) are computed but neither stored nor
 // reduced, which keeps the arithmetic free of per-site branches.
-template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true>
+// MAIN = false stores nothing: the stencil output of each site comes back in
+// ns_out, and the second output of the stage (Q of RK4 stage 2, K_m of
+// Cash-Karp stages 1-5) in aux_out, for callers that store neighbouring
+// sites together.
+template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true, bool MAIN = true>
 __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)[PY], const S (&pw)[PY][NPWX],
                                             const bool (&act)[PY], int i, const int (&j)[PY], int k,
                                             const long long (&o)[PY], int gz, const ColumnConsts (&cc)[PY],
-                                            double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr) {
+                                            double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr,
+                                            S* aux_out = nullptr) {
   using T = StageTraits<KIND>;
   const Geom& g = a.g;
   cx<C> lap[PY], c0[PY];
@@ -482,7 +500,9 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
           ns[q] = to_s<S>(cx<C>{base.r + (ar * f[q].r - ai * f[q].i), base.i + (ar * f[q].i + ai * f[q].r)});
         }
-        if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        if constexpr (MAIN) {
+          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        }
         if constexpr (KIND == K_RK4_2) {
           // Q = (psi + A) + h k2 in the stencil's compute type: Q is rounded
           // to S either way, and no third enters here (a C-rounded 1/3 would
@@ -498,7 +518,11 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
             qs = to_s<S>(cx<C>{(pc.r + c0[q].r) + (br * f[q].r - bi * f[q].i),
                                (pc.i + c0[q].i) + (br * f[q].i + bi * f[q].r)});
           }
-          if (act[q]) ((S*)a.acc)[o[q]] = qs;
+          if constexpr (MAIN) {
+            if (act[q]) ((S*)a.acc)[o[q]] = qs;
+          } else {
+            aux_out[q] = qs;
+          }
         }
       } else if constexpr (KIND != K_CK_6 && sizeof(C) != sizeof(double)) {
         // Cash-Karp stages 1-5 in the stencil's compute type: K_m = dt f and
@@ -506,7 +530,11 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
         const cx<C> Km{(C)a.cf_r[0] * f[q].r - (C)a.cf_i[0] * f[q].i,
                        (C)a.cf_r[0] * f[q].i + (C)a.cf_i[0] * f[q].r};
         const S Ks = to_s<S>(Km);
-        if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+        if constexpr (MAIN) {
+          if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+        } else {
+          aux_out[q] = Ks;
+        }
         const cx<C> Kmc = to_c<C>(Ks);
         const cx<C> pc = (KIND == K_CK_1) ? c0[q] : to_c<C>(pv);
         C tr = pc.r, ti = pc.i;
@@ -519,7 +547,9 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
         tr = tr + (C)a.b[T::NK] * Kmc.r;
         ti = ti + (C)a.b[T::NK] * Kmc.i;
         ns[q] = to_s<S>(cx<C>{tr, ti});
-        if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        if constexpr (MAIN) {
+          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+        }
       } else {
         // Cash-Karp stage m: K_m = dt * f ; tmp = psi + sum_j b_j K_j
         const cx<double> Km = cmuld(a.cf_r[0], a.cf_i[0], fd);
@@ -527,7 +557,11 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
         const cx<double> Kmd = to_c<double>(Ks);
         const cx<double> pd = (KIND == K_CK_1) ? cx<double>{cr, ci} : to_c<double>(pv);
         if constexpr (KIND != K_CK_6) {
-          if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+          if constexpr (MAIN) {
+            if (act[q]) ((S*)a.kout)[o[q]] = Ks;
+          } else {
+            aux_out[q] = Ks;
+          }
           double tr = pd.r, ti = pd.i;
 #pragma unroll
           for (int m = 0; m < T::NK; ++m) {
@@ -538,7 +572,9 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           tr = tr + a.b[T::NK] * Kmd.r;
           ti = ti + a.b[T::NK] * Kmd.i;
           ns[q] = to_s<S>(cx<double>{tr, ti});
-          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          if constexpr (MAIN) {
+            if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          }
         } else {
           // kin = K1, K3, K4, K5; c2 = c5 = 0 and dc2 = 0 (solve.f90:270-281)
           // contribute exact zeros and are skipped.
@@ -550,7 +586,9 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
           const double nr = (((pd.r + C1 * k1.r) + C3 * k3.r) + C4 * k4.r) + C6 * Kmd.r;
           const double ni = (((pd.i + C1 * k1.i) + C3 * k3.i) + C4 * k4.i) + C6 * Kmd.i;
           ns[q] = to_s<S>(cx<double>{nr, ni});
-          if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          if constexpr (MAIN) {
+            if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);
+          }
           const double er = (((DC1 * k1.r + DC3 * k3.r) + DC4 * k4.r) + DC5 * k5.r) + DC6 * Kmd.r;
           const double ei = (((DC1 * k1.i + DC3 * k3.i) + DC4 * k4.i) + DC5 * k5.i) + DC6 * Kmd.i;
           // psi_scal = |psi| + dt_entry |f| + 1e-30 (complex), |f| = |K1|/|dt|

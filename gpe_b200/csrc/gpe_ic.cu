@@ -77,15 +77,10 @@ __device__ __forceinline__ void ring_val(const gpe_ring& vr, double sc, double x
   *im = tr * z2i + ti * z2r;
 }
 
-template <class S>
-__global__ void k_ic_closed_form(S* f, Geom g, int R, int bcs, IcGrid G, gpe_ic ic) {
-  const long long n = (long long)g.nx * g.ny * g.nz;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % g.nx);
-    const long long rq = t / g.nx;
-    const int j = (int)(rq % g.ny);
-    const int k = (int)(rq / g.ny);
-    const double x = coord(G.xl, G.dx, i), y = coord(G.yl, G.dy, j), z = coord(G.zl, G.dz, k);
+// The product of the closed-form factors of ic at (x, y, z), factors taken
+// left to right as the reference's init_cond expression multiplies them.
+__device__ __forceinline__ void ic_product(const gpe_ic& ic, const IcGrid& G, double x, double y, double z,
+                                           double* out_r, double* out_i) {
     double pr = 1.0, pi = 0.0;
     for (int q = 0; q < ic.nfactors; ++q) {
       double fr = 1.0, fi = 0.0;
@@ -122,11 +117,56 @@ __global__ void k_ic_closed_form(S* f, Geom g, int R, int bcs, IcGrid G, gpe_ic 
       pr = nr;
       pi = ni;
     }
+    *out_r = pr;
+    *out_i = pi;
+}
+
+template <class S>
+__global__ void k_ic_closed_form(S* f, Geom g, int R, int bcs, IcGrid G, gpe_ic ic) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx);
+    const long long rq = t / g.nx;
+    const int j = (int)(rq % g.ny);
+    const int k = (int)(rq / g.ny);
+    const double x = coord(G.xl, G.dx, i), y = coord(G.yl, G.dy, j), z = coord(G.zl, G.dz, k);
+    double pr, pi;
+    ic_product(ic, G, x, y, z, &pr, &pi);
     S s;
     s.x = (typename Stor<S>::R)pr;
     s.y = (typename Stor<S>::R)pi;
     store_with_ghosts(f, g, (long long)(j + 2) * g.px + g.xoff + i, i, j, k, ghost_pos(i, g.nx, R, bcs),
                       ghost_pos(j, g.ny, R, bcs), ghost_pos(k, g.nz, R, bcs), s);
+  }
+}
+
+// psi <- psi * IC (modulus = 0: the state_restart product with init_cond,
+// src/ic.f90:160-162) or psi <- |psi| * IC (modulus = 1:
+// imprint_vortex_line, src/variables.f90:1166-1180), in FP64 per site, the
+// new value stored with its ghosts.
+template <class S>
+__global__ void k_ic_multiply(S* f, Geom g, int R, int bcs, IcGrid G, gpe_ic ic, int modulus) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % g.nx);
+    const long long rq = t / g.nx;
+    const int j = (int)(rq % g.ny);
+    const int k = (int)(rq / g.ny);
+    const double x = coord(G.xl, G.dx, i), y = coord(G.yl, G.dy, j), z = coord(G.zl, G.dz, k);
+    double pr, pi;
+    ic_product(ic, G, x, y, z, &pr, &pi);
+    const long long col = (long long)(j + 2) * g.px + g.xoff + i;
+    const S v = f[(long long)(k + 2) * g.pz + col];
+    double ar = (double)v.x, ai = (double)v.y;
+    if (modulus) {
+      ar = hypot(ar, ai);
+      ai = 0.0;
+    }
+    S s;
+    s.x = (typename Stor<S>::R)(ar * pr - ai * pi);
+    s.y = (typename Stor<S>::R)(ar * pi + ai * pr);
+    store_with_ghosts(f, g, col, i, j, k, ghost_pos(i, g.nx, R, bcs), ghost_pos(j, g.ny, R, bcs),
+                      ghost_pos(k, g.nz, R, bcs), s);
   }
 }
 
@@ -270,8 +310,7 @@ int ic_validate(const gpe_ic* ic, std::string& why) {
 
 bool ic_needs_fft(const gpe_ic* ic) { return ic->nfactors == 1 && ic->factor[0] == GPE_IC_RANDOM_PHASE; }
 
-cudaError_t ic_generate(const gpe_params& p, const Geom& g, int esz, int R, const gpe_ic& ic, void* psi_field,
-                        void* work, size_t work_bytes, cudaStream_t st) {
+IcGrid ic_grid(const gpe_params& p) {
   IcGrid G;
   G.nx = p.nx;
   G.ny = p.ny;
@@ -288,6 +327,22 @@ cudaError_t ic_generate(const gpe_params& p, const Geom& g, int esz, int R, cons
   G.omy = p.omy;
   G.omz = p.omz;
   G.scal = p.scal;
+  return G;
+}
+
+cudaError_t ic_multiply(const gpe_params& p, const Geom& g, int esz, int R, const gpe_ic& ic, void* psi_field,
+                        int modulus, cudaStream_t st) {
+  if (ic_needs_fft(&ic)) return cudaErrorInvalidValue;
+  const IcGrid G = ic_grid(p);
+  const int nb = 148 * 8;
+  if (esz == 16) k_ic_multiply<double2><<<nb, 256, 0, st>>>((double2*)psi_field, g, R, p.bcs, G, ic, modulus);
+  else k_ic_multiply<float2><<<nb, 256, 0, st>>>((float2*)psi_field, g, R, p.bcs, G, ic, modulus);
+  return cudaGetLastError();
+}
+
+cudaError_t ic_generate(const gpe_params& p, const Geom& g, int esz, int R, const gpe_ic& ic, void* psi_field,
+                        void* work, size_t work_bytes, cudaStream_t st) {
+  const IcGrid G = ic_grid(p);
   const int nb = 148 * 8;
   if (!ic_needs_fft(&ic)) {
     if (esz == 16) k_ic_closed_form<double2><<<nb, 256, 0, st>>>((double2*)psi_field, g, R, p.bcs, G, ic);

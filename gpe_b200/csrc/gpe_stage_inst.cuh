@@ -3,6 +3,9 @@
 //   cudaError_t launch_stage_<TAG>(int kind, int R, int ty, dim3 grid,
 //                                  cudaStream_t st, const StageArgs& a)
 #pragma once
+#include <cstdlib>
+#include <type_traits>
+
 #include "gpe_device.cuh"
 #include "gpe_stage_tma.cuh"
 
@@ -82,11 +85,63 @@ static cudaError_t launch_tma_kind(int kind, dim3 grid, cudaStream_t st, const T
   }
 }
 
+template <class C, int R, int K, int TY, int PY>
+static cudaError_t launch_tma_pair_one(dim3 grid, cudaStream_t st, const TmaMaps& m, const StageArgs& a) {
+  using LY = TmaLayout<float2, R, StageTraits<K>::NPW, TY>;
+  static unsigned long long attr_set = 0;  // per instantiation, one bit per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64 || !(attr_set & (1ULL << dev))) {
+    cudaError_t e = cudaFuncSetAttribute(k_stage_tma_pair<C, R, K, TY, PY>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
+    if (e != cudaSuccess) return e;
+    if (dev < 64) attr_set |= 1ULL << dev;
+  }
+  k_stage_tma_pair<C, R, K, TY, PY><<<grid, dim3(16, TY / PY), LY::SMEM, st>>>(m, a);
+  return cudaGetLastError();
+}
+
+template <class C, int R, int TY, int PY>
+static cudaError_t launch_tma_pair_kind(int kind, dim3 grid, cudaStream_t st, const TmaMaps& m,
+                                        const StageArgs& a) {
+  switch (kind) {
+#define GPE_PCASE(K) \
+  case K:            \
+    return launch_tma_pair_one<C, R, K, TY, PY>(grid, st, m, a);
+    GPE_PCASE(K_EULER)
+    GPE_PCASE(K_RK2_1)
+    GPE_PCASE(K_RK2_2)
+    GPE_PCASE(K_RK4_1)
+    GPE_PCASE(K_RK4_2)
+    GPE_PCASE(K_RK4_3)
+    GPE_PCASE(K_RK4_4)
+    GPE_PCASE(K_CK_1)
+    GPE_PCASE(K_CK_2)
+    GPE_PCASE(K_CK_3)
+    GPE_PCASE(K_CK_4)
+    GPE_PCASE(K_CK_5)
+    GPE_PCASE(K_CK_6)
+    GPE_PCASE(K_ENERGY)
+#undef GPE_PCASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 template <class S, class C>
 static cudaError_t launch_stage_tma_impl(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
                                          const StageArgs& a) {
-  // ty selects the rows per thread: 8 = one row per thread (256 threads),
-  // 4 = two rows per thread (128 threads); the tile is 32 x 8 either way
+  // ty is a TileVariant: TILE_32x8_ROW1 / TILE_32x8_ROW2 (any storage), or
+  // the pair layouts (complex64 storage with FP32 stencil compute)
+  if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
+    if (ty == TILE_PAIR_32x8) {
+      if (R == 1) return launch_tma_pair_kind<C, 1, 8, 1>(kind, grid, st, m, a);
+      if (R == 2) return launch_tma_pair_kind<C, 2, 8, 1>(kind, grid, st, m, a);
+    } else if (ty == TILE_PAIR_32x16) {
+      if (R == 1) return launch_tma_pair_kind<C, 1, 16, 2>(kind, grid, st, m, a);
+      if (R == 2) return launch_tma_pair_kind<C, 2, 16, 2>(kind, grid, st, m, a);
+    }
+  }
   if (ty == 8) {
     if (R == 1) return launch_tma_kind<S, C, 1, 8, 1>(kind, grid, st, m, a);
     if (R == 2) return launch_tma_kind<S, C, 2, 8, 1>(kind, grid, st, m, a);
@@ -97,9 +152,20 @@ static cudaError_t launch_stage_tma_impl(int kind, int R, int ty, dim3 grid, cud
   return cudaErrorInvalidValue;
 }
 
+// The batched kernel's thread layout for complex64 storage with the FP32
+// stencil: two x-adjacent sites per thread (GPE_BATCH_PAIR=0 selects the
+// one-site-per-column layout instead).
+inline bool batch_pair_layout() {
+  static const bool on = [] {
+    const char* e = getenv("GPE_BATCH_PAIR");
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
+}
+
 // Opt the batched kernel into its dynamic shared memory once per device and
 // cache how many of its CTAs fit on the device at once.
-template <class S, class C, int K>
+template <class S, class C, int K, bool PAIR>
 static cudaError_t batch_setup(int* occupancy) {
   using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
   static unsigned long long done = 0;
@@ -108,14 +174,13 @@ static cudaError_t batch_setup(int* occupancy) {
   cudaGetDevice(&dev);
   if (dev >= 64) return cudaErrorInvalidDevice;
   if (!(done & (1ULL << dev))) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_stage_batch<S, C, K, 8, BATCH_PY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)LY::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, 8, BATCH_PY, PAIR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8, BATCH_PY>, 256 / BATCH_PY,
-                                                      LY::SMEM);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8, BATCH_PY, PAIR>,
+                                                      256 / BATCH_PY, LY::SMEM);
     if (e != cudaSuccess) return e;
     occ[dev] = nsm * (per > 0 ? per : 1);
     done |= 1ULL << dev;
@@ -124,15 +189,29 @@ static cudaError_t batch_setup(int* occupancy) {
   return cudaSuccess;
 }
 
-template <class S, class C, int K>
+template <class S, class C, int K, bool PAIR>
 static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                                     const int* order, int nitems, int* queue, double* partials) {
   using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
-  cudaError_t e = batch_setup<S, C, K>(nullptr);
+  cudaError_t e = batch_setup<S, C, K, PAIR>(nullptr);
   if (e != cudaSuccess) return e;
-  k_stage_batch<S, C, K, 8, BATCH_PY><<<grid, dim3(32, 8 / BATCH_PY), LY::SMEM, st>>>(tab, items, order, nitems,
-                                                                                        queue, partials);
+  const dim3 block = PAIR ? dim3(16, 8) : dim3(32, 8 / BATCH_PY);
+  k_stage_batch<S, C, K, 8, BATCH_PY, PAIR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
+                                                                            partials);
   return cudaGetLastError();
+}
+
+template <class S, class C, int K>
+static cudaError_t launch_batch_kind(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+                                     const int* order, int nitems, int* queue, double* partials, int* occupancy) {
+  if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
+    if (batch_pair_layout()) {
+      if (grid <= 0) return batch_setup<S, C, K, true>(occupancy);
+      return launch_batch_one<S, C, K, true>(grid, st, tab, items, order, nitems, queue, partials);
+    }
+  }
+  if (grid <= 0) return batch_setup<S, C, K, false>(occupancy);
+  return launch_batch_one<S, C, K, false>(grid, st, tab, items, order, nitems, queue, partials);
 }
 
 template <class S, class C>
@@ -140,10 +219,9 @@ static cudaError_t launch_batch_impl(int kind, int grid, cudaStream_t st, const 
                                      const BatchItem* items, const int* order, int nitems, int* queue,
                                      double* partials, int* occupancy) {
   switch (kind) {
-#define GPE_BCASE(K)                                                       \
-  case K:                                                                  \
-    if (grid <= 0) return batch_setup<S, C, K>(occupancy);               \
-    return launch_batch_one<S, C, K>(grid, st, tab, items, order, nitems, queue, partials);
+#define GPE_BCASE(K) \
+  case K:            \
+    return launch_batch_kind<S, C, K>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
     GPE_BCASE(K_RK4_1)
     GPE_BCASE(K_RK4_2)
     GPE_BCASE(K_RK4_3)

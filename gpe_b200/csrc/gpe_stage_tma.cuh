@@ -405,6 +405,282 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
 }
 
 // ---------------------------------------------------------------------------
+// Two x-adjacent sites per thread, complex64 storage.  The 32 x TY tile is
+// processed by 16 x (TY/PY) threads; thread (tx, tyt) owns the sites
+// (2tx, 2tx+1) of rows tyt + r*TY/PY.  Every shared-memory read of the
+// stencil and point-wise tiles moves both sites of a pair (one 16-byte word),
+// so a pair takes three reads for its x neighbourhood and one per y
+// neighbour row instead of eight single-site reads per site, and the stage
+// outputs leave as 16-byte stores.  The per-site arithmetic is sites_stage,
+// the same as the one-site-per-column kernels, so results are identical.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 lds_pair(const float2* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+// store the sites (i, i+1) of a pair; i+1 inside the grid implies i is
+__device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool act0, bool act1) {
+  if (act1)
+    *reinterpret_cast<float4*>(p) = make_float4(v0.x, v0.y, v1.x, v1.y);
+  else if (act0)
+    *p = v0;
+}
+
+template <class C, int R, int KIND, int TY, int PY, class LY>
+__device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
+                                              TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
+                                              double& r_err) {
+  using S = float2;
+  using T = StageTraits<KIND>;
+  constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w(), TXT = TX / 2, TYT = TY / PY;
+  constexpr int NSS = LY::NSS, NPS = LY::NPS, NPW = T::NPW;
+  constexpr int NS = 2 * PY;  // sites per thread: site 2r + s is x = i0 + s of owned row r
+  constexpr uint32_t ST_BYTES = tma_st_bytes<S>(R, TY), PW1 = tma_pw1_bytes<S>(TY);
+  static_assert(TY % PY == 0, "PY must divide TY");
+  static_assert(HX % 2 == 0 && TW % 2 == 0, "pairs must stay 16-byte aligned in the tiles");
+
+  const Geom& g = a.g;
+  const int tx = threadIdx.x, tyt = threadIdx.y, tid = tyt * TXT + tx;
+  const int i0 = bx * TX + 2 * tx;
+  const int kb = bz * a.zc;
+  const int ke = min(kb + a.zc, g.nz);
+  const int M = ke - kb;
+  const int L = M + 2 * R;
+  const int SB = rg.sbase, PB = rg.pbase;
+
+  const int cxs = 2 * (g.xoff + bx * TX - HX);
+  const int cys = by * TY - R + 2;
+  const int cxp = 2 * (g.xoff + bx * TX);
+  const int cyp = by * TY + 2;
+
+  int issued_s = 0, issued_p = 0;
+  auto issue_stencil = [&](int l) {
+    const int G = SB + l, s = G % NSS;
+    mbar_arrive_expect_tx(&rg.sbar[s], ST_BYTES);
+    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, kb - R + l + 2);
+    issued_s = l + 1;
+  };
+  auto issue_pw = [&](int m) {
+    if constexpr (NPW > 0) {
+      const int G = PB + m, s = G % NPS;
+      mbar_arrive_expect_tx(&rg.pbar[s], NPW * PW1);
+#pragma unroll
+      for (int f = 0; f < NPW; ++f)
+        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, kb + m + 2);
+      issued_p = m + 1;
+    }
+  };
+  auto swait = [&](int l) { return mbar_wait_bounded(&rg.sbar[(SB + l) % NSS], ((SB + l) / NSS) & 1); };
+  auto pwait = [&](int m) { return mbar_wait_bounded(&rg.pbar[(PB + m) % NPS], ((PB + m) / NPS) & 1); };
+  auto drain = [&](int waited_s, int waited_p) {
+    if (tid == 0) {
+      atomicCAS(a.status, STATUS_OK, STATUS_WAIT_EXPIRED);  // a standing test value stays
+      for (int l = waited_s; l < issued_s; ++l) swait(l);
+      for (int m = waited_p; m < issued_p; ++m) pwait(m);
+    }
+    __syncthreads();
+  };
+
+  if (tid == 0) {
+    for (int l = 0; l < min(NSS, L); ++l) issue_stencil(l);
+    for (int m = 0; m < min(NPS, M); ++m) issue_pw(m);
+  }
+
+  int jr[PY], cofs[PY], pofs[PY], jq[NS];
+  bool act[NS];
+  long long o[PY], oq[NS];
+  ColumnConsts cc[NS];
+#pragma unroll
+  for (int r = 0; r < PY; ++r) {
+    const int ty = tyt + r * TYT;
+    jr[r] = by * TY + ty;
+    cofs[r] = (ty + R) * TW + 2 * tx + HX;
+    pofs[r] = ty * TX + 2 * tx;
+    o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i0;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int q = 2 * r + s;
+      act[q] = (i0 + s < g.nx) && (jr[r] < g.ny);
+      jq[q] = jr[r];
+      oq[q] = o[r] + s;
+      cc[q] = column_consts(a, i0 + s, jr[r], R, act[q]);
+    }
+  }
+  const bool xyg = (bx * TX <= R) || (bx * TX + TX - 1 >= g.nx - 1 - R) || (by * TY <= R) ||
+                   (by * TY + TY - 1 >= g.ny - 1 - R);
+
+  auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
+  float4 q[PY][2 * R + 1];  // z queue of each owned row's pair: planes k-R .. k+R
+  bool ok = true;
+  if (*(volatile const int*)a.status == STATUS_EXPIRE_TEST) ok = mbar_wait_bounded(rg.nbar, 0, EXPIRE_TEST_POLLS);
+#pragma unroll
+  for (int l = 0; l < 2 * R; ++l) {
+    ok &= swait(l);
+    const S* tl = stile(l);
+#pragma unroll
+    for (int r = 0; r < PY; ++r) q[r][l] = lds_pair(tl + cofs[r]);
+  }
+  if (!ok) *s_abort = 1;
+  __syncthreads();
+  if (*s_abort) {
+    drain(0, 0);
+    return false;
+  }
+  if (tid == 0) {
+    fence_proxy_async();
+    for (int l = 0; l < R; ++l)
+      if (l + NSS < L) issue_stencil(l + NSS);
+  }
+
+  int sl_s = (SB + 2 * R) % NSS, sl_p = ((SB + 2 * R) / NSS) & 1;
+  int sc_s = (SB + R) % NSS;
+  int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
+
+  for (int m = 0; m < M; ++m) {
+    const int k = kb + m;
+    const int lc = m + R, ll = m + 2 * R;
+    bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
+    {
+      const S* tl = (const S*)(rg.sring + sl_s * LY::ST_SLOT);
+#pragma unroll
+      for (int r = 0; r < PY; ++r) q[r][2 * R] = lds_pair(tl + cofs[r]);
+    }
+    const S* pws = nullptr;
+    if constexpr (NPW > 0) {
+      okw &= mbar_wait_bounded(&rg.pbar[pw_s], pw_p);
+      pws = (const S*)(rg.pring + pw_s * LY::PW_SLOT);
+    }
+    if (!okw) *s_abort = 1;
+
+    if (okw) {
+      const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
+      const int gz = (k <= R || k >= g.nz - 1 - R) ? zghost_pos(k, g.nz, R, a.bcs, a.zghost) : NOGHOST;
+      constexpr int NPWX = NPW > 0 ? NPW : 1;
+      Nb<C> n[NS];
+      S pv[NS][NPWX];
+#pragma unroll
+      for (int r = 0; r < PY; ++r) {
+        const S* c = tile + cofs[r];
+        const float4 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = q[r][R];
+        const float4 ym1 = lds_pair(c - TW), yp1 = lds_pair(c + TW);
+        Nb<C>& n0 = n[2 * r];
+        Nb<C>& n1 = n[2 * r + 1];
+        n0.c0 = to_c<C>(lo2(cc4));
+        n1.c0 = to_c<C>(hi2(cc4));
+        n0.xm1 = to_c<C>(hi2(xl));
+        n0.xp1 = to_c<C>(hi2(cc4));
+        n1.xm1 = to_c<C>(lo2(cc4));
+        n1.xp1 = to_c<C>(lo2(xr));
+        n0.ym1 = to_c<C>(lo2(ym1));
+        n1.ym1 = to_c<C>(hi2(ym1));
+        n0.yp1 = to_c<C>(lo2(yp1));
+        n1.yp1 = to_c<C>(hi2(yp1));
+        n0.zm1 = to_c<C>(lo2(q[r][R - 1]));
+        n1.zm1 = to_c<C>(hi2(q[r][R - 1]));
+        n0.zp1 = to_c<C>(lo2(q[r][R + 1]));
+        n1.zp1 = to_c<C>(hi2(q[r][R + 1]));
+        if constexpr (R == 2) {
+          const float4 ym2 = lds_pair(c - 2 * TW), yp2 = lds_pair(c + 2 * TW);
+          n0.xm2 = to_c<C>(lo2(xl));
+          n1.xm2 = to_c<C>(hi2(xl));
+          n0.xp2 = to_c<C>(lo2(xr));
+          n1.xp2 = to_c<C>(hi2(xr));
+          n0.ym2 = to_c<C>(lo2(ym2));
+          n1.ym2 = to_c<C>(hi2(ym2));
+          n0.yp2 = to_c<C>(lo2(yp2));
+          n1.yp2 = to_c<C>(hi2(yp2));
+          n0.zm2 = to_c<C>(lo2(q[r][0]));
+          n1.zm2 = to_c<C>(hi2(q[r][0]));
+          n0.zp2 = to_c<C>(lo2(q[r][4]));
+          n1.zp2 = to_c<C>(hi2(q[r][4]));
+        } else {
+          n0.xm2 = n0.xp2 = n0.ym2 = n0.yp2 = n0.zm2 = n0.zp2 = cx<C>{0, 0};
+          n1.xm2 = n1.xp2 = n1.ym2 = n1.yp2 = n1.zm2 = n1.zp2 = cx<C>{0, 0};
+        }
+#pragma unroll
+        for (int f = 0; f < NPW; ++f) {
+          const float4 w = lds_pair(pws + f * (TX * TY) + pofs[r]);
+          pv[2 * r][f] = lo2(w);
+          pv[2 * r + 1][f] = hi2(w);
+        }
+      }
+      S ns[NS], ax[NS];
+      sites_stage<S, C, R, KIND, NS, NPWX, false, false, false>(a, n, pv, act, i0, jq, k, oq, gz, cc, r_norm,
+                                                                 r_en, r_err, ns, ax);
+      if constexpr (KIND != K_ENERGY) {
+        S* out = (S*)a.out;
+#pragma unroll
+        for (int r = 0; r < PY; ++r) st_pair(out + o[r], ns[2 * r], ns[2 * r + 1], act[2 * r], act[2 * r + 1]);
+        if constexpr (KIND == K_RK4_2) {
+#pragma unroll
+          for (int r = 0; r < PY; ++r)
+            st_pair((S*)a.acc + o[r], ax[2 * r], ax[2 * r + 1], act[2 * r], act[2 * r + 1]);
+        }
+        if constexpr (KIND >= K_CK_1 && KIND <= K_CK_5) {
+#pragma unroll
+          for (int r = 0; r < PY; ++r)
+            st_pair((S*)a.kout + o[r], ax[2 * r], ax[2 * r + 1], act[2 * r], act[2 * r + 1]);
+        }
+        // face ghosts after the sites, in uniform branches (see tma_item)
+        if (xyg) {
+#pragma unroll
+          for (int q2 = 0; q2 < NS; ++q2)
+            if (act[q2]) {
+              const long long os = o[q2 / 2] + (q2 & 1);
+              if (cc[q2].gx != NOGHOST) out[os + (cc[q2].gx - (i0 + (q2 & 1)))] = ns[q2];
+              if (cc[q2].gy != NOGHOST) out[os + (long long)(cc[q2].gy - jr[q2 / 2]) * g.px] = ns[q2];
+            }
+        }
+        if (gz != NOGHOST) {
+          const long long zo = (long long)(gz - k) * g.pz;
+#pragma unroll
+          for (int r = 0; r < PY; ++r)
+            st_pair(out + o[r] + zo, ns[2 * r], ns[2 * r + 1], act[2 * r], act[2 * r + 1]);
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < PY; ++r) {
+#pragma unroll
+      for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
+      o[r] += g.pz;
+    }
+    if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
+    if (++sc_s == NSS) sc_s = 0;
+    if (++pw_s == NPS) { pw_s = 0; pw_p ^= 1; }
+
+    __syncthreads();
+    if (*s_abort) {
+      drain(ll, m);
+      return false;
+    }
+    if (tid == 0) {
+      fence_proxy_async();
+      if (lc + NSS < L) issue_stencil(lc + NSS);
+      if (m + NPS < M) issue_pw(m + NPS);
+    }
+  }
+  rg.sbase = SB + L;
+  rg.pbase = PB + (NPW > 0 ? M : 0);
+  return true;
+}
+
+// Single-solve stage kernel with two x-adjacent sites per thread
+// (complex64 storage): one work item per CTA, 16 x TY/PY threads.
+template <class C, int R, int KIND, int TY, int PY>
+__global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_constant__ TmaMaps maps,
+                                                                const StageArgs a) {
+  using LY = TmaLayout<float2, R, StageTraits<KIND>::NPW, TY>;
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ int s_abort;
+  TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
+  double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+  if (!tma_item_pair<C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+                                             r_en, r_err))
+    return;
+  if (a.partials) block_reduce_store<16 * TY / PY>(r_norm, r_en, r_err, a.partials);
+}
+
+// ---------------------------------------------------------------------------
 // Batched, persistent stage kernel: many independent solves (any sizes, BCs,
 // orders 2 and 4) advanced by one launch per stage.  Work item w = tile
 // (bx, by, bz) of solve items[w].solve.  CTAs take items from a work queue:
@@ -439,17 +715,22 @@ __host__ __device__ constexpr int batch_min_blocks() {
                                                                                      : 1;
 }
 
-template <class S, class C, int KIND, int TY, int PY>
+// PAIR (complex64 storage with the FP32 stencil only): 16 x 8 threads, each
+// with two x-adjacent sites of one row of the 32 x 8 item tile
+// (tma_item_pair); otherwise 32 x TY/PY threads with PY rows each.
+template <class S, class C, int KIND, int TY, int PY, bool PAIR = false>
 __global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k_stage_batch(const BatchStage* __restrict__ tab,
                                                          const BatchItem* __restrict__ items,
                                                          const int* __restrict__ order, int nitems,
                                                          int* queue, double* partials) {
+  static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && 32 * TY / PY == 16 * TY),
+                "the pair layout is for complex64 / FP32 with one row per thread");
   using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ int s_w[2];  // item taken from the queue, double-buffered by turn parity
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
-  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   int fenced = -1;  // solve whose tensor maps thread 0 has acquired (they do not change within a launch)
   for (int turn = 0;; ++turn) {
     if (tid == 0) {
@@ -473,12 +754,21 @@ __global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k
     const int R = sa.R;
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;
-    if (R == 1)
-      ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                               r_err);
-    else
-      ok = tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                               r_err);
+    if constexpr (PAIR) {
+      if (R == 1)
+        ok = tma_item_pair<C, 1, KIND, TY, 1, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                  r_err);
+      else
+        ok = tma_item_pair<C, 2, KIND, TY, 1, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                  r_err);
+    } else {
+      if (R == 1)
+        ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                 r_err);
+      else
+        ok = tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                 r_err);
+    }
     if (!ok) return;
     if (partials) block_reduce_store_at<32 * TY / PY>(r_norm, r_en, r_err, partials, w);
   }

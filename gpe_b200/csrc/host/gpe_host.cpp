@@ -489,11 +489,59 @@ void end_state(Ctx& c, bool final_) {
   join_writer(c);
   const auto b = state_bytes(c);
   write_end_state(c, meta(c), b.data(), b.size());
+  if (c.r.save_filter) {
+    // the final filtered state (end_state flag 1 -> filtered_surface flag 1,
+    // src/io.f90:870-873, 598-607): the input of a saved_restart
+    mkdir(path("proc0000").c_str(), 0755);
+    const std::string name = "proc0000/end_state_filtered.dat";
+    std::vector<char> fb(b.size());
+    check(c, gpe_filtered(c.h, 1.0, c.r.filter_kc, fb.data(), c.esz == 16 ? GPE_C128 : GPE_C64));
+    FILE* f = fopen(path(name).c_str(), "wb");
+    if (!f) emergency_stop("ERROR: cannot write " + name);
+    for (int v : {c.P.nx, c.P.ny, c.P.nz, (int)c.p}) wr_int(f, v);
+    wr_real(f, c, c.t);
+    wr_real(f, c, c.im_t);
+    wr_real(f, c, c.dt.real());
+    wr_real(f, c, c.dt.imag());
+    fwrite(fb.data(), 1, fb.size(), f);
+    fclose(f);
+  }
   unlink(path("RUNNING").c_str());
 }
 
+// proc0000/end_state_filtered.dat as state_restart reads it with
+// saved_restart (src/ic.f90:144-157): four integers and two reals are
+// skipped, then nx*ny*nz complex values are read.  The writer
+// (filtered_surface, src/io.f90:598-607) puts the complex dt between t, im_t
+// and the field, so the reference's reader takes dt as the first element and
+// drops the field's last one; read the same way, for the same state.
+std::vector<std::complex<double>> read_saved_filtered(const Ctx& c) {
+  const std::string name = "proc0000/end_state_filtered.dat";
+  FILE* f = fopen(path(name).c_str(), "rb");
+  if (!f) emergency_stop("ERROR: saved_restart=.true. but " + name + " does not exist.");
+  const size_t n = (size_t)c.P.nx * c.P.ny * c.P.nz;
+  const size_t rs = c.esz / 2;  // bytes of one real
+  std::vector<char> b(n * c.esz);
+  bool ok = fseek(f, (long)(4 * 4 + 2 * rs), SEEK_SET) == 0 && fread(b.data(), 1, b.size(), f) == b.size();
+  fclose(f);
+  if (!ok) emergency_stop("ERROR: " + name + " is truncated");
+  std::vector<std::complex<double>> v(n);
+  for (size_t q = 0; q < n; ++q) {
+    if (c.esz == 16) {
+      double w[2];
+      memcpy(w, b.data() + q * 16, 16);
+      v[q] = {w[0], w[1]};
+    } else {
+      float w[2];
+      memcpy(w, b.data() + q * 8, 8);
+      v[q] = {w[0], w[1]};
+    }
+  }
+  return v;
+}
+
 // state_restart (src/ic.f90:117-191) from end_state0000.dat
-void state_restart(Ctx& c) {
+void state_restart(Ctx& c, const gpe_ic& ic) {
   FILE* f = fopen(path("end_state0000.dat").c_str(), "rb");
   if (!f) emergency_stop("ERROR: restart=.true. but end_state0000.dat does not exist.");
   int32_t n[4];
@@ -525,7 +573,28 @@ void state_restart(Ctx& c) {
   }
   if (c.r.scheme == "rk45") c.dt = dtp;
   else if (dtp != c.dt) c.p = (int64_t)((double)c.p * std::abs(dtp) / std::abs(c.dt));
+  // state_restart = out_var1 * out_var2 * init_cond (src/ic.f90:164):
+  // out_var2 = the saved filtered state (saved_restart) else 1, init_cond =
+  // the ic.in product (multiply_ic_restart) else 1; products taken left to
+  // right with the naive complex multiply, the last one on the device
+  if (c.r.saved_restart) {
+    const auto f2 = read_saved_filtered(c);
+    for (size_t q = 0; q < f2.size(); ++q) {
+      if (c.esz == 16) {
+        double* a = (double*)(b.data() + q * 16);
+        const double ar = a[0], ai = a[1];
+        a[0] = ar * f2[q].real() - ai * f2[q].imag();
+        a[1] = ar * f2[q].imag() + ai * f2[q].real();
+      } else {
+        float* a = (float*)(b.data() + q * 8);
+        const float ar = a[0], ai = a[1], br = (float)f2[q].real(), bi = (float)f2[q].imag();
+        a[0] = ar * br - ai * bi;
+        a[1] = ar * bi + ai * br;
+      }
+    }
+  }
   check(c, gpe_set_state(c.h, b.data(), c.esz == 16 ? GPE_C128 : GPE_C64));
+  if (c.r.multiply_ic_restart) check(c, gpe_multiply_ic(c.h, &ic, 0));
 }
 
 // itos (src/io.f90:29-47): the last seven digits of n, zero-padded
@@ -676,6 +745,7 @@ int main(int argc, char** argv) {
            ic.ring.r0, ic.ring.plane[0], ic.ring.plane[1], ic.line.x0, ic.line.dir);
     return 0;
   }
+  if (c.r.imprint_vl && !c.P.have_vl1) emergency_stop("ERROR: imprint_vl=.true. but parameters.in has no vl1");
   FILE* run = fopen(path("RUNNING").c_str(), "w");
   if (run) fclose(run);
   if (gpe_create(&p, &c.h) != GPE_OK) emergency_stop(std::string("ERROR: ") + gpe_last_error(nullptr));
@@ -685,7 +755,7 @@ int main(int argc, char** argv) {
   c.z.resize(p.nz);
   double dxyz[3];
   gpe_get_grid(c.h, c.x.data(), c.y.data(), c.z.data(), dxyz);
-  if (c.r.restart) state_restart(c);
+  if (c.r.restart) state_restart(c, ic);
   else {
     if (exists("end_state0000.dat")) emergency_stop("ERROR: restart=.false. but end_state0000.dat exists.");
     check(c, gpe_set_ic(c.h, &ic));
@@ -701,6 +771,45 @@ int main(int argc, char** argv) {
   const double nsites = (double)p.nx * p.ny * p.nz;
   int64_t ps = (int64_t)(c.t / c.r.p_save), n2 = (int64_t)(c.t / c.r.save_rate2);
   int64_t m3 = (int64_t)(c.t / c.r.save_rate3);
+  gpe_ic imprint{};
+  imprint.nfactors = 1;
+  imprint.factor[0] = GPE_IC_LINE;
+  imprint.line = c.P.vl1;
+  // Fixed-step real-time runs advance in chunks of up to kChunk steps per
+  // gpe_step call (one replayed step graph per step, no host round trip in
+  // between).  A chunk ends before any step at whose start the reference's
+  // loop does something besides stepping (a save or diagnostic whose test
+  // fires, the end of the loop), and at every step after which the norm is
+  // needed (eqn 4: a norm record after it or after the next step, whose
+  // relnorm needs this one).  The clock is advanced here exactly as the
+  // library advances it (t += Re dt, im_t += |Im dt|), so the chunk ends are
+  // the reference's event steps.  RUNNING and SAVE are polled once per chunk.
+  const int64_t kChunk = 100;
+  struct Clk {
+    double t, im_t;
+  };
+  const auto advance = [&](Clk k) { return Clk{k.t + c.dt.real(), k.im_t + std::fabs(c.dt.imag())}; };
+  const auto save_step = [&](Clk k) {  // modulo(t+im_t, |dt| save_rate) < |dt|
+    const double adt = std::abs(c.dt);
+    return fmodulo(k.t + k.im_t, adt * c.r.save_rate) < adt;
+  };
+  const auto pre_event = [&](Clk k) {  // anything at the top of the reference's loop besides stepping
+    const double tt = k.t + k.im_t;
+    return !(tt <= c.r.end_time) || save_step(k) || tt >= c.r.save_rate3 * m3 || tt >= c.r.save_rate2 * n2 ||
+           tt >= c.r.p_save * ps;
+  };
+  const bool eq4 = c.r.eqn == 4;
+  const auto chunk_len = [&]() -> int64_t {
+    if (c.r.scheme == "rk45" || !c.r.real_time) return 1;
+    Clk k{c.t, c.im_t};
+    for (int64_t n = 1; n < kChunk; ++n) {
+      const Clk k1 = advance(k), k2 = advance(k1);
+      if (eq4 && (save_step(k1) || save_step(k2))) return n;  // the norm after step n-1 is needed
+      if (pre_event(k1)) return n;
+      k = k1;
+    }
+    return kChunk;
+  };
   while (c.t + c.im_t <= c.r.end_time) {
     if (!exists("RUNNING")) {  // src/gpe.f90:137-161
       printf("\n Stop requested.\n");
@@ -726,6 +835,7 @@ int main(int argc, char** argv) {
       end_state(c, false);
       ++ps;
     }
+    const int64_t nstep = chunk_len();
     gpe_step_info io;
     memset(&io, 0, sizeof(io));
     io.t = c.t;
@@ -733,11 +843,23 @@ int main(int argc, char** argv) {
     io.dt_re = c.dt.real();
     io.dt_im = c.dt.imag();
     io.p = c.p;
-    io.want_norm = c.r.eqn == 4 ? 1 : 0;
-    check(c, gpe_step(c.h, 1, &io));
+    // eqn 4 forms the norm of the new state (src/gpe.f90:243-249): every
+    // step in imaginary time and with RKF45; in fixed-step real time only
+    // where a record or the next record's relnorm uses it
+    io.want_norm = eq4 ? 1 : 0;
+    if (eq4 && c.r.real_time && c.r.scheme != "rk45") {
+      // the norm of the chunk's last step is needed iff a norm record
+      // follows it or the step after it
+      Clk k{c.t, c.im_t};
+      for (int64_t q = 0; q < nstep; ++q) k = advance(k);
+      io.want_norm = (save_step(k) || save_step(advance(k))) ? 1 : 0;
+    }
+    check(c, gpe_step(c.h, nstep, &io));
+    const double norm_before = io.norm;
     c.t = io.t;
     c.im_t = io.im_t;
     c.dt = std::complex<double>(io.dt_re, io.dt_im);
+    c.p += nstep - 1;  // the last step's index; incremented at the end of the pass
     if (c.r.scheme == "rk45" && c.p % c.r.save_rate == 0)  // src/solve.f90:234-241
       append_line("timestep.dat", fe(c.t) + fe(c.im_t) + fe(std::abs(c.dt)) + [&] {
         char b[16];
@@ -748,13 +870,13 @@ int main(int argc, char** argv) {
       idl_surface(c);
       unlink(path("SAVE").c_str());
     }
-    if (c.r.eqn == 4) {  // src/gpe.f90:243-249
-      norm = io.norm;
+    if (eq4 && io.want_norm) {  // src/gpe.f90:243-249
+      norm = norm_before;
       relnorm = std::fabs((norm - prev_norm) / prev_norm);
       if (fmodulo(c.t + c.im_t, std::abs(c.dt) * c.r.save_rate) < std::abs(c.dt))
         append_line("norm.dat", fe(c.t) + fe(c.im_t) + fe(norm) + fe(relnorm));
     }
-    if (c.r.eqn == 4 && !c.r.real_time) {  // src/gpe.f90:253-273
+    if (eq4 && !c.r.real_time) {  // src/gpe.f90:253-273
       if (relnorm < 1e-12) {
         if (c.r.stop_imag) break;  // End run if stop after imaginary time requested
         c.r.real_time = true;
@@ -767,8 +889,9 @@ int main(int argc, char** argv) {
         printf(" Switching to real time\n");
       }
       if (c.r.renorm) check(c, gpe_renormalise(c.h, norm));
+      if (c.r.imprint_vl) check(c, gpe_multiply_ic(c.h, &imprint, 1));  // src/gpe.f90:272
     }
-    prev_norm = norm;
+    if (eq4 && io.want_norm) prev_norm = norm;
     ++c.p;
   }
   end_state(c, true);

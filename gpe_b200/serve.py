@@ -1,9 +1,11 @@
 """Serving loop: a stream of Gross-Pitaevskii solve requests served by one
 GPU with continuous batching.
 
-Requests arrive over time (Poisson), are admitted into a Pool as soon as
-their state fits in the HBM budget, join the running batch at the next chunk
-boundary, and leave with their final state when done.  Latency of a request
+Requests arrive over time (Poisson), are admitted into a Pool -- shortest
+job first among those that have arrived, as long as their state fits in the
+HBM budget and the sites in flight stay under a cap -- join the running
+batch at the next chunk boundary, and leave with their final state when
+done.  Latency of a request
 = completion time - arrival time (host clock).  Nothing here waits for the
 batch to drain before admitting new work.
 """
@@ -114,17 +116,20 @@ class ServeReport:
 
 
 def serve(requests: list[Request], budget_bytes: int, chunk: int = 50, realtime: bool = True,
-          prep_threads: int = 4, device_ics: bool = True, max_active_sites: int = 160 << 20,
-          on_result=None) -> ServeReport:
+          prep_threads: int = 4, device_ics: bool = True, max_active_sites: int = 48 << 20,
+          on_result=None, policy: str = "sjf") -> ServeReport:
     """Run the request stream through one Pool.  With realtime=True a request
     becomes visible at its arrival time on the host clock; every loop turn
     admits what has arrived and fits, advances the batch by up to `chunk`
     steps, and collects finished solves.  device_ics=True builds each
     initial state on the GPU at admission; False prepares it on host
     threads and copies it in.  on_result(request, result), if given, sees
-    every finished solve before its result buffer is reused."""
+    every finished solve before its result buffer is reused.  policy (device
+    ICs): "sjf" admits the arrived requests with the least work (sites x
+    steps) first, "fcfs" in arrival order; either way up to
+    max_active_sites grid sites in flight."""
     if device_ics:
-        return _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result)
+        return _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result, policy)
     pool = Pool(budget_bytes)
     rep = ServeReport()
     pending = sorted(requests, key=lambda r: r.arrival_s)
@@ -195,11 +200,18 @@ def _storage_dtype(params) -> np.dtype:
     return np.dtype(np.complex64 if params.storage == "c64" else np.complex128)
 
 
-def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result=None) -> ServeReport:
-    """Admission is first-come first-served, bounded by the HBM budget and by
-    max_active_sites: enough grid sites in flight to keep the GPU's memory
-    system busy, no more, so that early requests are not slowed by every
-    later arrival."""
+def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites, on_result=None,
+                      policy: str = "sjf") -> ServeReport:
+    """Admission is bounded by the HBM budget and by max_active_sites: enough
+    grid sites in flight to keep the GPU's memory system busy, no more, so
+    that admitted requests are not slowed by every later arrival.  Among the
+    arrived requests, "sjf" admits the one with the least work first (a
+    solve in the pool runs to completion, so this is shortest-job-first
+    without preemption): short requests no longer queue behind long ones,
+    which is what sets the median latency under load; "fcfs" keeps arrival
+    order."""
+    if policy not in ("sjf", "fcfs"):
+        raise ValueError("policy must be 'sjf' or 'fcfs'")
     pool = Pool(budget_bytes)
     rep = ServeReport()
     bufs = ResultBuffers()
@@ -215,10 +227,12 @@ def _serve_device_ics(requests, budget_bytes, chunk, realtime, max_active_sites,
         while nxt < len(pending) and (not realtime or pending[nxt].arrival_s <= now):
             waiting.append(pending[nxt])
             nxt += 1
+        if policy == "sjf":
+            waiting.sort(key=lambda r: (r.sites * r.nsteps, r.arrival_s))
         still = []
         for q, req in enumerate(waiting):
             if active and active_sites + req.sites > max_active_sites:
-                still.extend(waiting[q:])  # first come, first served
+                still.extend(waiting[q:])  # the head of the order waits for room
                 break
             p = req.params
             out = bufs.get((p.nz, p.ny, p.nx), _storage_dtype(p))

@@ -190,6 +190,11 @@ class Solver:
         """Generate the initial state on the device (see ic.device_spec)."""
         _check(self.lib, self.h, self.lib.gpe_set_ic(self.h, C.byref(spec)))
 
+    def multiply_ic(self, spec, modulus: bool = False) -> None:
+        """psi <- psi * IC, or |psi| * IC with modulus (imprint_vortex_line,
+        src/variables.f90:1166-1180), on the device."""
+        _check(self.lib, self.h, self.lib.gpe_multiply_ic(self.h, C.byref(spec), 1 if modulus else 0))
+
     # -- stepping -----------------------------------------------------------
     def solver(self, nsteps: int = 1, want_norm: bool = False, want_energy: bool = False,
                wait: bool = True) -> L.GpeStepInfo:

@@ -202,6 +202,14 @@ typedef struct {
 /* Set the handle's state to the initial condition (no host array). */
 int gpe_set_ic(gpe_handle* h, const gpe_ic* ic);
 
+/* Multiply the current state by an initial-condition product, on the device
+ * in FP64 per site: modulus = 0 gives psi <- psi * IC, the restart product
+ * with ic.in of state_restart (src/ic.f90:160-162, multiply_ic_restart);
+ * modulus = 1 gives psi <- |psi| * IC, imprint_vortex_line
+ * (src/variables.f90:1166-1180, imprint_vl, applied at src/gpe.f90:272).
+ * Closed-form factors only (a random-phase factor is GPE_ERR_BADARG). */
+int gpe_multiply_ic(gpe_handle* h, const gpe_ic* ic, int32_t modulus);
+
 /* FFT diagnostics of the current state, computed on the device in FP64
  * (cuFFT), with the reference's transform a = DFT(psi)/sqrt(nx ny nz)
  * (src/ic.f90:910-939).

@@ -10,6 +10,7 @@ import pytest
 from gpe_b200 import ic
 from gpe_b200.pool import Pool
 from gpe_b200.solver import RunParams, Solver
+from oracle.pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -78,6 +79,14 @@ def test_pool_mix_equals_alone_bitwise(gpu):
         assert r.norm == pytest.approx(s.get_norm(), rel=1e-12)
         if rp.scheme == "rk45":
             assert r.dt == s.dt
+        # and directly against the FP64 CPU oracle on the same initial state
+        o = Oracle(rp.replace(storage="c128"))
+        oref = o.run(state(rp, i).astype(np.complex128), steps)
+        err = np.linalg.norm(r.psi - oref) / np.linalg.norm(oref)
+        if rp.storage == "c64":
+            assert err <= 1e-5
+        else:
+            assert err <= (1e-10 if rp.scheme == "rk45" else 1e-12)
 
 
 def test_pool_budget_admission(gpu):

@@ -8,8 +8,9 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from gpe_b200.serve import device_ic, make_requests, serve
+from gpe_b200.serve import device_ic, initial_state, make_requests, serve
 from gpe_b200.solver import Solver
+from oracle.pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -36,3 +37,13 @@ def test_served_results_equal_single_handles(gpu):
         alone = s.get_state(np.complex64 if req.params.storage == "c64" else np.complex128)
         s.close()
         np.testing.assert_array_equal(psi, alone)
+        # and against the FP64 CPU oracle from the host restatement of the
+        # request's initial state
+        rp64 = req.params.replace(storage="c128")
+        psi0 = initial_state(req.__class__(**{**req.__dict__, "params": rp64}))
+        oref = Oracle(rp64).run(psi0, req.nsteps)
+        err = np.linalg.norm(psi - oref) / np.linalg.norm(oref)
+        if req.params.storage == "c64":
+            assert err <= 1e-5
+        else:
+            assert err <= (1e-10 if req.params.scheme == "rk45" else 1e-12)

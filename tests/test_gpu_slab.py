@@ -11,6 +11,7 @@ import pytest
 from gpe_b200 import _lib as L
 from gpe_b200 import ic, slab
 from gpe_b200.solver import RunParams, Solver
+from oracle.pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +55,11 @@ def test_hub_slabs_match_whole_grid(gpu, name, nslabs):
     assert np.array_equal(out, ref)
     assert norm == pytest.approx(ref_norm, rel=1e-13)
     assert t == ref_t
+    # and directly against the CPU oracle (the reference's single-rank path)
+    o = Oracle(rp)
+    oref = o.run(psi, 12)
+    assert np.linalg.norm(out - oref) / np.linalg.norm(oref) <= 1e-12
+    assert norm == pytest.approx(o.get_norm(oref), rel=1e-12)
 
 
 @pytest.mark.parametrize("storage", ["c128", "c64"])
@@ -66,6 +72,12 @@ def test_hub_slabs_rk45_same_step_control(gpu, storage):
     assert np.array_equal(out, ref)
     assert t == ref_t  # same t, im_t, dt and p: every slab took the same decisions
     assert norm == pytest.approx(ref_norm, rel=1e-13)
+    # against the FP64 CPU oracle: adaptive-step tolerance for complex128,
+    # the FP32-storage bar for complex64
+    o = Oracle(rp.replace(storage="c128"))
+    oref = o.run(psi, 8)
+    err = np.linalg.norm(out - oref) / np.linalg.norm(oref)
+    assert err <= (1e-10 if storage == "c128" else 1e-5)
 
 
 def test_hub_energy_and_norm_calls(gpu):

@@ -50,11 +50,16 @@ def test_expired_wait_reports_timeout_and_handle_recovers(gpu, scheme, storage):
     s.set_state(psi0)
     s.solver(6)
     out = s.get_state()
-    ref = Oracle(rp.replace(storage="c128", compute="auto")).run(psi0, 6)
+    # exactly what a fresh handle computes
+    f = Solver(rp)
+    f.set_state(psi0)
+    f.solver(6)
+    np.testing.assert_array_equal(out, f.get_state())
+    assert (s.t, s.dt) == (f.t, f.dt)
+    f.close()
     if storage == "c128":
+        ref = Oracle(rp).run(psi0, 6)
         assert rel_l2(out, ref) <= (1e-10 if scheme == "rk45" else 1e-12)
-    else:
-        assert rel_l2(out, ref) <= 1e-5
     s.close()
 
 

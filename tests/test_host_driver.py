@@ -60,3 +60,15 @@ def test_missing_namelist_is_an_emergency_stop(ring_dir):
     r = run_host(ring_dir, "--parse-only")
     assert r.returncode != 0
     assert "error reading namelist misc_params" in (ring_dir / "ERROR").read_text()
+
+
+def test_imprint_without_a_vortex_line_is_an_emergency_stop(ring_dir):
+    t = (ring_dir / "run.in").read_text().replace("imprint_vl          = .false.", "imprint_vl          = .true.")
+    (ring_dir / "run.in").write_text(t)
+    pin = (ring_dir / "parameters.in").read_text()
+    start = pin.index("  type (line_param)")
+    end = pin.index("  type (ring_param)")
+    (ring_dir / "parameters.in").write_text(pin[:start] + pin[end:])
+    r = run_host(ring_dir)
+    assert r.returncode != 0
+    assert "imprint_vl=.true. but parameters.in has no vl1" in (ring_dir / "ERROR").read_text()
