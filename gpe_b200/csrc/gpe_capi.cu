@@ -67,7 +67,9 @@ struct gpe_handle {
   double dx = 0, dy = 0, dz = 0;
   double* part_a = nullptr;  // block partials (energy / first reduction)
   double* part_b = nullptr;  // block partials (norm / errmax)
-  long long npart = 0;
+  long long npart = 0;       // partials of one stage launch (one per CTA of grid)
+  dim3 norm_grid;            // k_norm's grid: 32 x 8 tiles x z-chunks
+  long long norm_npart = 0;  // its partials
   double* dres = nullptr;    // [6] finalised reductions
   double* hres = nullptr;    // pinned mirror of dres
   void* staging = nullptr;
@@ -324,8 +326,8 @@ StageArgs base_args(gpe_handle* h) {
   return a;
 }
 
-int finalize_into(gpe_handle* h, const double* part, int slot) {
-  k_finalize<<<1, 256, 0, h->st>>>(part, h->npart, h->dres + 3 * slot);
+int finalize_into(gpe_handle* h, const double* part, int slot, long long nparts = -1) {
+  k_finalize<<<1, 256, 0, h->st>>>(part, nparts < 0 ? h->npart : nparts, h->dres + 3 * slot);
   CU(h, cudaGetLastError());
   return GPE_OK;
 }
@@ -529,13 +531,13 @@ int norm_now(gpe_handle* h, double* out) {
   const size_t ntot = (size_t)h->p.nx + h->p.ny + h->p.nz;
   const double* w = h->tables + 2 * ntot;
   if (h->esz == 16)
-    k_norm<double2><<<h->grid, dim3(32, 8), 0, h->st>>>((const double2*)h->fields[h->cur], g, h->zc, w, w + g.nx,
-                                                        w + g.nx + g.ny, h->part_b);
+    k_norm<double2><<<h->norm_grid, dim3(32, 8), 0, h->st>>>((const double2*)h->fields[h->cur], g, h->zc, w,
+                                                             w + g.nx, w + g.nx + g.ny, h->part_b);
   else
-    k_norm<float2><<<h->grid, dim3(32, 8), 0, h->st>>>((const float2*)h->fields[h->cur], g, h->zc, w, w + g.nx,
-                                                       w + g.nx + g.ny, h->part_b);
+    k_norm<float2><<<h->norm_grid, dim3(32, 8), 0, h->st>>>((const float2*)h->fields[h->cur], g, h->zc, w,
+                                                            w + g.nx, w + g.nx + g.ny, h->part_b);
   CU(h, cudaGetLastError());
-  if (int rc = finalize_into(h, h->part_b, 1)) return rc;
+  if (int rc = finalize_into(h, h->part_b, 1, h->norm_npart)) return rc;
   if (int rc = fetch_results(h)) return rc;
   *out = ((h->hres[3] * h->dx) * h->dy) * h->dz;
   return GPE_OK;
@@ -689,6 +691,9 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
   h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g, th);
   h->grid = dim3((pl.nx + 31) / 32, (pl.ny + th - 1) / th, (pl.nz + h->zc - 1) / h->zc);
   h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
+  h->norm_grid = dim3((pl.nx + 31) / 32, (pl.ny + 7) / 8, (pl.nz + h->zc - 1) / h->zc);
+  h->norm_npart = (long long)h->norm_grid.x * h->norm_grid.y * h->norm_grid.z;
+  const long long npart_alloc = std::max(h->npart, h->norm_npart);
   auto bail = [&](int rc) {
     std::string m = h->err;
     gpe_destroy(h);
@@ -730,8 +735,8 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
   std::vector<double> tab;
   build_tables(h, tab);
   if (cudaMalloc(&h->tables, tab.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->part_a, h->npart * RED_SLOTS * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&h->part_b, h->npart * RED_SLOTS * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->part_a, npart_alloc * RED_SLOTS * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->part_b, npart_alloc * RED_SLOTS * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&h->dres, 6 * sizeof(double)) != cudaSuccess ||
       cudaMallocHost(&h->hres, 6 * sizeof(double)) != cudaSuccess) {
     cudaGetLastError();

@@ -172,6 +172,7 @@ def test_chunked_real_time_norm_records(gpu, tmp_path):
     """Real-time fixed-step runs are stepped in chunks; the norm records
     (t, im_t, norm, relnorm at the save steps, relnorm against the previous
     step's norm) are those of stepping one step at a time."""
+    from gpe_b200 import ic
     from gpe_b200.solver import Solver
 
     nx, xr, tau, end_time, save_rate = 24, 5.75, 0.01, 1.0, 7
@@ -181,9 +182,8 @@ def test_chunked_real_time_norm_records(gpu, tmp_path):
     run(d)
     recs = [[float(v) for v in line.split()] for line in (d / "norm.dat").read_text().splitlines()]
     rp = params(nx, xr, tau).replace(order=4, bcs=1)
-    o = Oracle(rp)
     s = Solver(rp)
-    s.set_state(o.fermi() * o.vortex_line(x0=0.3, y0=-0.2, dir="z"))
+    s.set_ic(ic.device_spec("fermi", "line", line=dict(x0=0.3, y0=-0.2)))  # the driver's device IC
     want, prev, t = [], 1.0, 0.0
     while t <= end_time:
         info = s.solver(1, want_norm=True)

@@ -80,13 +80,17 @@ def test_pool_mix_equals_alone_bitwise(gpu):
         if rp.scheme == "rk45":
             assert r.dt == s.dt
         # and directly against the FP64 CPU oracle on the same initial state
-        o = Oracle(rp.replace(storage="c128"))
-        oref = o.run(state(rp, i).astype(np.complex128), steps)
-        err = np.linalg.norm(r.psi - oref) / np.linalg.norm(oref)
-        if rp.storage == "c64":
-            assert err <= 1e-5
-        else:
-            assert err <= (1e-10 if rp.scheme == "rk45" else 1e-12)
+        # (not RKF45 with complex64 storage: its step sizes differ from the
+        # FP64 oracle's, so equal step counts are different times; that case
+        # is compared at matched times in test_gpu_parity.py)
+        if not (rp.scheme == "rk45" and rp.storage == "c64"):
+            o = Oracle(rp.replace(storage="c128"))
+            oref = o.run(state(rp, i).astype(np.complex128), steps)
+            err = np.linalg.norm(r.psi - oref) / np.linalg.norm(oref)
+            if rp.storage == "c64":
+                assert err <= 1e-5
+            else:
+                assert err <= (1e-10 if rp.scheme == "rk45" else 1e-12)
 
 
 def test_pool_budget_admission(gpu):

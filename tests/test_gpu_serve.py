@@ -38,7 +38,10 @@ def test_served_results_equal_single_handles(gpu):
         s.close()
         np.testing.assert_array_equal(psi, alone)
         # and against the FP64 CPU oracle from the host restatement of the
-        # request's initial state
+        # request's initial state (not RKF45 with complex64 storage: its
+        # step sizes differ from the FP64 oracle's, see test_gpu_parity.py)
+        if req.params.scheme == "rk45" and req.params.storage == "c64":
+            continue
         rp64 = req.params.replace(storage="c128")
         psi0 = initial_state(req.__class__(**{**req.__dict__, "params": rp64}))
         oref = Oracle(rp64).run(psi0, req.nsteps)

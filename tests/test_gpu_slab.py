@@ -72,12 +72,13 @@ def test_hub_slabs_rk45_same_step_control(gpu, storage):
     assert np.array_equal(out, ref)
     assert t == ref_t  # same t, im_t, dt and p: every slab took the same decisions
     assert norm == pytest.approx(ref_norm, rel=1e-13)
-    # against the FP64 CPU oracle: adaptive-step tolerance for complex128,
-    # the FP32-storage bar for complex64
-    o = Oracle(rp.replace(storage="c128"))
-    oref = o.run(psi, 8)
-    err = np.linalg.norm(out - oref) / np.linalg.norm(oref)
-    assert err <= (1e-10 if storage == "c128" else 1e-5)
+    # against the FP64 CPU oracle over the first step, which both take with
+    # the same dt (later step sizes depend on error estimates that cancel to
+    # ~1e-6 of K, near the vortex core to rounding noise)
+    out1, _, _ = slab.step_decomposed(rp, psi, 3, 1)
+    oref = Oracle(rp.replace(storage="c128")).run(psi, 1)
+    err = np.linalg.norm(out1 - oref) / np.linalg.norm(oref)
+    assert err <= (1e-13 if storage == "c128" else 1e-6)
 
 
 def test_hub_energy_and_norm_calls(gpu):

@@ -57,7 +57,10 @@ def test_pair_layouts_equal_row_layout_bitwise(gpu, shape, order, bcs, scheme):
     for layout in ("pair_32x8", "pair_32x16"):
         out, info, e = run_with(layout, rp, psi0, 6, want_norm=True, want_energy=True)
         np.testing.assert_array_equal(out, ref)
-        assert info.norm == iref.norm and info.energy == iref.energy and e == eref
+        # the per-CTA partial sums follow the tile shape, so the reductions
+        # are the same sums in another order
+        assert info.norm == pytest.approx(iref.norm, rel=1e-13)
+        assert info.energy == pytest.approx(iref.energy, rel=1e-13) and e == pytest.approx(eref, rel=1e-13)
         assert (info.dt_re, info.dt_im, info.t) == (iref.dt_re, iref.dt_im, iref.t)
 
 
