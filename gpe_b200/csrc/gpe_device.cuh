@@ -296,20 +296,25 @@ struct Nb {
   cx<C> c0, xm1, xp1, xm2, xp2, ym1, yp1, ym2, yp2, zm1, zp1, zm2, zp2;
 };
 
-// Per-column constants hoisted out of the z loop.
+// Per-column constants hoisted out of the z loop, in the stencil's compute
+// type C (the FP32 stencil keeps them as floats: fewer registers per site).
+template <class C>
 struct ColumnConsts {
-  double wxy, vxy, sxy, rxy2;
-  float vh;  // 0.5 (vx + vy) rounded once, for FP32 compute
-  int gx, gy;
+  double wxy;  // norm quadrature weight wx wy
+  C vc;        // trap: vx + vy (FP64), or 0.5 (vx + vy) rounded once (FP32)
+  C sxy;       // sponge: sx + sy
+  C rxy2;      // sphere: x^2 + y^2
+  int gx, gy;  // x / y ghost positions (ghost_pos)
 };
 
-__device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i, int j, int R, bool active) {
-  ColumnConsts c;
+template <class C>
+__device__ __forceinline__ ColumnConsts<C> column_consts(const StageArgs& a, int i, int j, int R, bool active) {
+  ColumnConsts<C> c;
   c.wxy = active ? a.wx[i] * a.wy[j] : 0.0;
-  c.vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
-  c.vh = (float)(0.5 * c.vxy);
-  c.sxy = (active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0;
-  c.rxy2 = (active && a.eqn == 3) ? a.cx[i] * a.cx[i] + a.cy[j] * a.cy[j] : 0.0;
+  const double vxy = (active && a.eqn == 4) ? a.vx[i] + a.vy[j] : 0.0;
+  c.vc = sizeof(C) == sizeof(double) ? (C)vxy : (C)(0.5 * vxy);
+  c.sxy = (C)((active && a.has_diss) ? a.sx[i] + a.sy[j] : 0.0);
+  c.rxy2 = (C)((active && a.eqn == 3) ? a.cx[i] * a.cx[i] + a.cy[j] * a.cy[j] : 0.0);
   c.gx = ghost_pos(i, a.g.nx, R, a.bcs);
   c.gy = ghost_pos(j, a.g.ny, R, a.bcs);
   return c;
@@ -322,7 +327,7 @@ __device__ __forceinline__ ColumnConsts column_consts(const StageArgs& a, int i,
 // the sums keep the reference's left-to-right order.
 template <class C, int PY>
 __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY], const cx<C> (&lap)[PY],
-                                         const cx<C> (&dpx)[PY], const ColumnConsts (&cc)[PY], int k,
+                                         const cx<C> (&dpx)[PY], const ColumnConsts<C> (&cc)[PY], int k,
                                          cx<C> (&r)[PY]) {
   C n2[PY];
 #pragma unroll
@@ -338,8 +343,8 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
 #pragma unroll
     for (int q = 0; q < PY; ++q) {
       C v;
-      if constexpr (sizeof(C) == sizeof(double)) v = (C)(0.5 * (cc[q].vxy + vz));
-      else v = cc[q].vh + vzh;
+      if constexpr (sizeof(C) == sizeof(double)) v = (C)(0.5 * (cc[q].vc + vz));
+      else v = cc[q].vc + vzh;
       const C wr = ((-(C)0.5 * lap[q].r + v * p[q].r) + g * (n2[q] * p[q].r)) - mu * p[q].r;
       const C wi = ((-(C)0.5 * lap[q].i + v * p[q].i) + g * (n2[q] * p[q].i)) - mu * p[q].i;
       r[q].r = wi - gm * wr;
@@ -369,7 +374,12 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
     if (a.has_diss) {
       const double sz = a.sz[k];
 #pragma unroll
-      for (int q = 0; q < PY; ++q) dd[q] = (C)(0.5 * (a.diss_amp * (cc[q].sxy + sz)));
+      if constexpr (sizeof(C) == sizeof(double)) {
+        for (int q = 0; q < PY; ++q) dd[q] = 0.5 * (a.diss_amp * (cc[q].sxy + sz));
+      } else {
+        const C amp = (C)a.diss_amp, szf = (C)sz;
+        for (int q = 0; q < PY; ++q) dd[q] = (C)0.5 * (amp * (cc[q].sxy + szf));
+      }
     }
 #pragma unroll
     for (int q = 0; q < PY; ++q) {
@@ -390,7 +400,13 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
       const double zz = a.cz[k];
 #pragma unroll
       for (int q = 0; q < PY; ++q) {
-        const C sp = (C)(0.5 * (1.0 + tanh((sqrt(cc[q].rxy2 + zz * zz) - 10.0) - 2.0)));
+        C sp;
+        if constexpr (sizeof(C) == sizeof(double)) {
+          sp = 0.5 * (1.0 + tanh((sqrt(cc[q].rxy2 + zz * zz) - 10.0) - 2.0));
+        } else {
+          const C zf = (C)zz;
+          sp = (C)0.5 * ((C)1 + tanhf((sqrtf(cc[q].rxy2 + zf * zf) - (C)10) - (C)2));
+        }
         r[q].r *= sp;
         r[q].i *= sp;
       }
@@ -398,65 +414,67 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
   }
 }
 
-// Everything a stage does at the PY interior sites (i, j_q, k) of one thread
-// once their stencil neighbourhoods and point-wise inputs are in registers:
-// Laplacian, GP right-hand side, the stage combination, the stores (with
-// ghosts) and the fused reductions.  pw[q][] holds site q's point-wise
-// inputs in the order psi, acc, K... of StageTraits; o[q] is the element
-// offset of (i, j_q, k); gz = ghost_pos(k, nz, R, bcs).  Sites with
-// act[q] false (outside the grid) are computed but neither stored nor
-// reduced, which keeps the arithmetic free of per-site branches.
-// MAIN = false stores nothing: the stencil output of each site comes back in
-// ns_out, and the second output of the stage (Q of RK4 stage 2, K_m of
-// Cash-Karp stages 1-5) in aux_out, for callers that store neighbouring
-// sites together.
-template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true, bool MAIN = true>
-__device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)[PY], const S (&pw)[PY][NPWX],
-                                            const bool (&act)[PY], int i, const int (&j)[PY], int k,
-                                            const long long (&o)[PY], int gz, const ColumnConsts (&cc)[PY],
-                                            double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr,
-                                            S* aux_out = nullptr) {
-  using T = StageTraits<KIND>;
-  const Geom& g = a.g;
-  cx<C> lap[PY], c0[PY];
+// Laplacian of one site from its neighbourhood.  FP64: the reference's
+// expression order (derivs.f90:164-181, then laplacian = dxx + dyy + dzz,
+// variables.f90:55-71).  FP32 stencil: each axis's bracket keeps the
+// reference's order, so the cancellation of a smooth field happens inside it
+// at the scale of one axis, and the three brackets are scaled and summed with
+// one multiply and two fused multiply-adds, (iz Dz + (iy Dy + ix Dx)): 15
+// instead of 17 operations per component.
+template <class C, int R>
+__device__ __forceinline__ cx<C> site_lap(const StageArgs& a, const Nb<C>& b) {
+  cx<C> lap;
   if constexpr (sizeof(C) == sizeof(double)) {
-    // FP64: the reference's expression order (derivs.f90:164-181, then
-    // laplacian = dxx + dyy + dzz, variables.f90:55-71)
-#pragma unroll
-    for (int q = 0; q < PY; ++q) {
-      const cx<C> lxx = d2<C, R>(n[q].xm2, n[q].xm1, n[q].c0, n[q].xp1, n[q].xp2, (C)a.ixx);
-      const cx<C> lyy = d2<C, R>(n[q].ym2, n[q].ym1, n[q].c0, n[q].yp1, n[q].yp2, (C)a.iyy);
-      const cx<C> lzz = d2<C, R>(n[q].zm2, n[q].zm1, n[q].c0, n[q].zp1, n[q].zp2, (C)a.izz);
-      lap[q].r = (lxx.r + lyy.r) + lzz.r;
-      lap[q].i = (lxx.i + lyy.i) + lzz.i;
-      c0[q] = n[q].c0;
-    }
+    const cx<C> lxx = d2<C, R>(b.xm2, b.xm1, b.c0, b.xp1, b.xp2, (C)a.ixx);
+    const cx<C> lyy = d2<C, R>(b.ym2, b.ym1, b.c0, b.yp1, b.yp2, (C)a.iyy);
+    const cx<C> lzz = d2<C, R>(b.zm2, b.zm1, b.c0, b.zp1, b.zp2, (C)a.izz);
+    lap.r = (lxx.r + lyy.r) + lzz.r;
+    lap.i = (lxx.i + lyy.i) + lzz.i;
   } else {
-    // FP32 stencil: each axis's bracket keeps the reference's order, so the
-    // cancellation of a smooth field happens inside it at the scale of one
-    // axis, and the three brackets are scaled and summed with one multiply
-    // and two fused multiply-adds: (iz Dz + (iy Dy + ix Dx)), 15 instead of
-    // 17 operations per component
     const C ix = (C)a.ixx, iy = (C)a.iyy, iz = (C)a.izz;
     auto axis = [](C m2, C m1, C c, C p1, C p2) -> C {
       if constexpr (R == 1) return (p1 - (C)2 * c) + m1;
       else return ((((-p2 + (C)16 * p1) - (C)30 * c) + (C)16 * m1) - m2);
     };
-#pragma unroll
-    for (int q = 0; q < PY; ++q) {
-      const Nb<C>& b = n[q];
-      const C dxr = axis(b.xm2.r, b.xm1.r, b.c0.r, b.xp1.r, b.xp2.r);
-      const C dxi = axis(b.xm2.i, b.xm1.i, b.c0.i, b.xp1.i, b.xp2.i);
-      const C dyr = axis(b.ym2.r, b.ym1.r, b.c0.r, b.yp1.r, b.yp2.r);
-      const C dyi = axis(b.ym2.i, b.ym1.i, b.c0.i, b.yp1.i, b.yp2.i);
-      const C dzr = axis(b.zm2.r, b.zm1.r, b.c0.r, b.zp1.r, b.zp2.r);
-      const C dzi = axis(b.zm2.i, b.zm1.i, b.c0.i, b.zp1.i, b.zp2.i);
-      lap[q].r = fmaf(iz, dzr, fmaf(iy, dyr, ix * dxr));
-      lap[q].i = fmaf(iz, dzi, fmaf(iy, dyi, ix * dxi));
-      c0[q] = b.c0;
-    }
+    const C dxr = axis(b.xm2.r, b.xm1.r, b.c0.r, b.xp1.r, b.xp2.r);
+    const C dxi = axis(b.xm2.i, b.xm1.i, b.c0.i, b.xp1.i, b.xp2.i);
+    const C dyr = axis(b.ym2.r, b.ym1.r, b.c0.r, b.yp1.r, b.yp2.r);
+    const C dyi = axis(b.ym2.i, b.ym1.i, b.c0.i, b.yp1.i, b.yp2.i);
+    const C dzr = axis(b.zm2.r, b.zm1.r, b.c0.r, b.zp1.r, b.zp2.r);
+    const C dzi = axis(b.zm2.i, b.zm1.i, b.c0.i, b.zp1.i, b.zp2.i);
+    lap.r = fmaf(iz, dzr, fmaf(iy, dyr, ix * dxr));
+    lap.i = fmaf(iz, dzi, fmaf(iy, dyi, ix * dxi));
   }
+  return lap;
+}
 
+// First x-derivative of one site (only read when Urhs != 0).
+template <class C, int R>
+__device__ __forceinline__ cx<C> site_dpx(const StageArgs& a, const Nb<C>& b) {
+  return d1<C, R>(b.xm2, b.xm1, b.xp1, b.xp2, (C)a.ix1);
+}
+
+// Everything a stage does at the PY interior sites (i, j_q, k) of one thread
+// once their Laplacians (lap), x-derivatives (dpx, read only when Urhs != 0),
+// centre values (c0) and point-wise inputs are in registers: GP right-hand
+// side, the stage combination, the stores (with ghosts) and the fused
+// reductions.  pw[q][] holds site q's point-wise inputs in the order psi,
+// acc, K... of StageTraits; o[q] is the element offset of (i, j_q, k);
+// gz = ghost_pos(k, nz, R, bcs).  Sites with act[q] false (outside the grid)
+// are computed but neither stored nor reduced, which keeps the arithmetic
+// free of per-site branches.  MAIN = false stores nothing: the stencil
+// output of each site comes back in ns_out, and the second output of the
+// stage (Q of RK4 stage 2, K_m of Cash-Karp stages 1-5) in aux_out, for
+// callers that store neighbouring sites together.
+template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true, bool MAIN = true>
+__device__ __forceinline__ void sites_update(const StageArgs& a, const cx<C> (&lap)[PY], const cx<C> (&c0)[PY],
+                                             const cx<C> (&dpx_in)[PY], const S (&pw)[PY][NPWX],
+                                             const bool (&act)[PY], int i, const int (&j)[PY], int k,
+                                             const long long (&o)[PY], int gz, const ColumnConsts<C> (&cc)[PY],
+                                             double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr,
+                                             S* aux_out = nullptr) {
+  using T = StageTraits<KIND>;
+  const Geom& g = a.g;
   if constexpr (T::FIRST) {
     if (a.want_energy) {
       // real(-lap * conjg(psi) + 0.5 |psi|^4)   (variables.f90:591-592)
@@ -470,14 +488,8 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
     }
   }
   if constexpr (KIND != K_ENERGY) {
-    cx<C> dpx[PY], f[PY];
-#pragma unroll
-    for (int q = 0; q < PY; ++q) dpx[q] = cx<C>{0, 0};
-    if (a.has_urhs) {
-#pragma unroll
-      for (int q = 0; q < PY; ++q) dpx[q] = d1<C, R>(n[q].xm2, n[q].xm1, n[q].xp1, n[q].xp2, (C)a.ix1);
-    }
-    gp_rhs_n<C, PY>(a, c0, lap, dpx, cc, k, f);
+    cx<C> f[PY];
+    gp_rhs_n<C, PY>(a, c0, lap, dpx_in, cc, k, f);
     S* out = (S*)a.out;
     constexpr bool FINAL = (KIND == K_EULER || KIND == K_RK2_2 || KIND == K_RK4_4 || KIND == K_CK_6);
     S ns[PY];  // the stored stencil output of each site
@@ -646,10 +658,32 @@ __device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)
   }
 }
 
+// sites_update from the PY sites' stencil neighbourhoods.
+template <class S, class C, int R, int KIND, int PY, int NPWX, bool GXY = true, bool GZ = true, bool MAIN = true>
+__device__ __forceinline__ void sites_stage(const StageArgs& a, const Nb<C> (&n)[PY], const S (&pw)[PY][NPWX],
+                                            const bool (&act)[PY], int i, const int (&j)[PY], int k,
+                                            const long long (&o)[PY], int gz, const ColumnConsts<C> (&cc)[PY],
+                                            double& r_norm, double& r_en, double& r_err, S* ns_out = nullptr,
+                                            S* aux_out = nullptr) {
+  cx<C> lap[PY], c0[PY], dpx[PY];
+#pragma unroll
+  for (int q = 0; q < PY; ++q) {
+    lap[q] = site_lap<C, R>(a, n[q]);
+    c0[q] = n[q].c0;
+    dpx[q] = cx<C>{0, 0};
+  }
+  if (a.has_urhs) {
+#pragma unroll
+    for (int q = 0; q < PY; ++q) dpx[q] = site_dpx<C, R>(a, n[q]);
+  }
+  sites_update<S, C, R, KIND, PY, NPWX, GXY, GZ, MAIN>(a, lap, c0, dpx, pw, act, i, j, k, o, gz, cc, r_norm, r_en,
+                                                       r_err, ns_out, aux_out);
+}
+
 // Single-site form (one site per thread).
 template <class S, class C, int R, int KIND>
 __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, const S* pw, int i, int j, int k,
-                                           long long o, int gz, const ColumnConsts& cc, double& r_norm,
+                                           long long o, int gz, const ColumnConsts<C>& cc, double& r_norm,
                                            double& r_en, double& r_err) {
   constexpr int NPWX = StageTraits<KIND>::NPW > 0 ? StageTraits<KIND>::NPW : 1;
   const Nb<C> nn[1] = {n};
@@ -659,7 +693,7 @@ __device__ __forceinline__ void site_stage(const StageArgs& a, const Nb<C>& n, c
   const bool act[1] = {true};
   const int jj[1] = {j};
   const long long oo[1] = {o};
-  const ColumnConsts c1[1] = {cc};
+  const ColumnConsts<C> c1[1] = {cc};
   sites_stage<S, C, R, KIND, 1, NPWX>(a, nn, pv, act, i, jj, k, oo, gz, c1, r_norm, r_en, r_err);
 }
 
@@ -718,7 +752,7 @@ __global__ void __launch_bounds__(32 * TY) k_stage(const StageArgs a) {
     hsm[h] = (p < NH) ? hy * TW + hx : 0;
     hcol[h] = (long long)(gj + 2) * g.px + g.xoff + gi;
   }
-  const ColumnConsts cc = column_consts(a, i, j, R, active);
+  const ColumnConsts<C> cc = column_consts<C>(a, i, j, R, active);
 
   // point-wise input pointers in StageTraits order
   const S* pwp[NPW];

@@ -243,7 +243,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   int jr[PY], cofs[PY];
   bool act[PY];
   long long o[PY];  // element offset of (i, j, k)
-  ColumnConsts cc[PY];
+  ColumnConsts<C> cc[PY];
 #pragma unroll
   for (int r = 0; r < PY; ++r) {
     const int ty = tyt + r * TYT;
@@ -251,7 +251,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     act[r] = (i < g.nx) && (jr[r] < g.ny);
     cofs[r] = (ty + R) * TW + tx + HX;
     o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i;
-    cc[r] = column_consts(a, i, jr[r], R, act[r]);
+    cc[r] = column_consts<C>(a, i, jr[r], R, act[r]);
   }
   // does this tile hold a site with an x or y ghost?  Ghosts come from the
   // index ranges [0, R] and [n-1-R, n-1] of an axis only.
@@ -488,7 +488,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
   int jr[PY], cofs[PY], pofs[PY], jq[NS];
   bool act[NS];
   long long o[PY], oq[NS];
-  ColumnConsts cc[NS];
+  ColumnConsts<C> cc[NS];
 #pragma unroll
   for (int r = 0; r < PY; ++r) {
     const int ty = tyt + r * TYT;
@@ -502,7 +502,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
       act[q] = (i0 + s < g.nx) && (jr[r] < g.ny);
       jq[q] = jr[r];
       oq[q] = o[r] + s;
-      cc[q] = column_consts(a, i0 + s, jr[r], R, act[q]);
+      cc[q] = column_consts<C>(a, i0 + s, jr[r], R, act[q]);
     }
   }
   const bool xyg = (bx * TX <= R) || (bx * TX + TX - 1 >= g.nx - 1 - R) || (by * TY <= R) ||
@@ -555,15 +555,17 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
       const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
       const int gz = (k <= R || k >= g.nz - 1 - R) ? zghost_pos(k, g.nz, R, a.bcs, a.zghost) : NOGHOST;
       constexpr int NPWX = NPW > 0 ? NPW : 1;
-      Nb<C> n[NS];
+      // each row's neighbourhoods are reduced to Laplacians (and, with
+      // Urhs, x-derivatives) right after its loads, so only one row's
+      // neighbours are live at a time
+      cx<C> lap[NS], c0[NS], dpx[NS];
       S pv[NS][NPWX];
 #pragma unroll
       for (int r = 0; r < PY; ++r) {
         const S* c = tile + cofs[r];
         const float4 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = q[r][R];
         const float4 ym1 = lds_pair(c - TW), yp1 = lds_pair(c + TW);
-        Nb<C>& n0 = n[2 * r];
-        Nb<C>& n1 = n[2 * r + 1];
+        Nb<C> n0, n1;
         n0.c0 = to_c<C>(lo2(cc4));
         n1.c0 = to_c<C>(hi2(cc4));
         n0.xm1 = to_c<C>(hi2(xl));
@@ -596,6 +598,15 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
           n0.xm2 = n0.xp2 = n0.ym2 = n0.yp2 = n0.zm2 = n0.zp2 = cx<C>{0, 0};
           n1.xm2 = n1.xp2 = n1.ym2 = n1.yp2 = n1.zm2 = n1.zp2 = cx<C>{0, 0};
         }
+        lap[2 * r] = site_lap<C, R>(a, n0);
+        lap[2 * r + 1] = site_lap<C, R>(a, n1);
+        c0[2 * r] = n0.c0;
+        c0[2 * r + 1] = n1.c0;
+        dpx[2 * r] = dpx[2 * r + 1] = cx<C>{0, 0};
+        if (a.has_urhs) {
+          dpx[2 * r] = site_dpx<C, R>(a, n0);
+          dpx[2 * r + 1] = site_dpx<C, R>(a, n1);
+        }
 #pragma unroll
         for (int f = 0; f < NPW; ++f) {
           const float4 w = lds_pair(pws + f * (TX * TY) + pofs[r]);
@@ -604,8 +615,8 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
         }
       }
       S ns[NS], ax[NS];
-      sites_stage<S, C, R, KIND, NS, NPWX, false, false, false>(a, n, pv, act, i0, jq, k, oq, gz, cc, r_norm,
-                                                                 r_en, r_err, ns, ax);
+      sites_update<S, C, R, KIND, NS, NPWX, false, false, false>(a, lap, c0, dpx, pv, act, i0, jq, k, oq, gz, cc,
+                                                                  r_norm, r_en, r_err, ns, ax);
       if constexpr (KIND != K_ENERGY) {
         S* out = (S*)a.out;
 #pragma unroll
