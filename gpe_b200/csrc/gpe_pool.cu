@@ -34,6 +34,9 @@ cudaError_t launch_batch_f32(int kind, int grid, cudaStream_t st, const BatchSta
                              const int* order, int nitems, int* queue, double* partials, int* occupancy);
 cudaError_t launch_batch_f32x(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                               const int* order, int nitems, int* queue, double* partials, int* occupancy);
+int batch_rows_f64(int kind);
+int batch_rows_f32(int kind);
+int batch_rows_f32x(int kind);
 }  // namespace gpe
 
 using namespace gpe;
@@ -100,6 +103,7 @@ struct Solve {
   double* tables = nullptr;
   double d[3] = {};
   int zc = 8, ntx = 1, nty = 1, ntz = 1;
+  int tile_h = 8;  // rows of the solve's 32-column work items (its class's kernel layout)
   int64_t nsteps = 0, done = 0, rejected = 0, quota = 0;
   double t = 0, im_t = 0, dr = 0, di = 0, dte_r = 0, dte_i = 0, errmax = 0, norm = 0;
   int64_t p_index = 0;
@@ -238,6 +242,16 @@ cudaError_t launch_batch(int cmode, int kind, int grid, cudaStream_t st, const B
   }
 }
 
+// rows of the work items of a (precision, scheme family) class
+int batch_rows(int cmode, int fam) {
+  const int kind = fam == FAM_RK45 ? K_CK_1 : K_RK4_1;
+  switch (cmode) {
+    case CM_F64: return batch_rows_f64(kind);
+    case CM_F32: return batch_rows_f32(kind);
+    default: return batch_rows_f32x(kind);
+  }
+}
+
 int grid_for(int cmode, int kind, int nitems) {
   int occ = 0;
   launch_batch(cmode, kind, 0, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, &occ);
@@ -371,7 +385,7 @@ int build_items(gpe_pool* P, Class& c, const std::vector<Solve*>& sv) {
     const BatchItem& it = c.hitems[w];
     const Solve* s = sv[it.solve];
     const int m = std::min(s->zc, s->g.nz - it.bz * s->zc);
-    const int cols = std::min(32, s->g.nx - it.bx * 32), rows = std::min(8, s->g.ny - it.by * 8);
+    const int cols = std::min(32, s->g.nx - it.bx * 32), rows = std::min(s->tile_h, s->g.ny - it.by * s->tile_h);
     cost[w] = (double)(m + 2 * s->R) * cols * rows;
   }
   c.horder.resize(c.hitems.size());
@@ -651,8 +665,9 @@ static int pool_submit_impl(gpe_pool* P, const gpe_params* prm, const void* psi0
   // default.  In a batch the other solves fill the GPU, so items can be long
   // (fewer z-halo re-reads per plane) instead of many.
   s->zc = prm->tile_zc > 0 ? std::min(prm->tile_zc, prm->nz) : std::min(prm->nz, prm->nz <= 48 ? 16 : 32);
+  s->tile_h = batch_rows(s->cmode, s->fam);
   s->ntx = (prm->nx + 31) / 32;
-  s->nty = (prm->ny + 7) / 8;
+  s->nty = (prm->ny + s->tile_h - 1) / s->tile_h;
   s->ntz = (prm->nz + s->zc - 1) / s->zc;
   s->field_bytes = Arena::round((size_t)padded_elems(s->g) * s->esz);
   s->bytes = s->field_bytes * s->nf + Arena::round(tables_bytes(*prm));
@@ -670,7 +685,7 @@ static int pool_submit_impl(gpe_pool* P, const gpe_params* prm, const void* psi0
     return pfail(P, rc, m);
   };
   for (int f = 0; f < s->nf; ++f)
-    if (!encode_maps(s->f[f], s->g, s->esz, s->R, &s->halo[f], &s->pw[f]))
+    if (!encode_maps(s->f[f], s->g, s->esz, s->R, &s->halo[f], &s->pw[f], s->tile_h))
       return bail(GPE_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   std::vector<double> tab;
   std::vector<double> xs, ys, zs;

@@ -163,24 +163,39 @@ inline bool batch_pair_layout() {
   return on;
 }
 
+// Item rows of the batched RK4 kernels for complex64 storage with the FP32
+// stencil: 32 x 16 items with the pair layout (two rows per thread), unless
+// GPE_BATCH_ROWS=8.  Every other class uses 32 x 8 items.
+inline int batch_rk4_f32_rows() {
+  static const int rows = [] {
+    const char* e = getenv("GPE_BATCH_ROWS");
+    return (e && atoi(e) == 8) || !batch_pair_layout() ? 8 : 16;
+  }();
+  return rows;
+}
+
+__host__ __device__ constexpr bool is_rk4_kind(int k) {
+  return k == K_RK4_1 || k == K_RK4_2 || k == K_RK4_3 || k == K_RK4_4;
+}
+
 // Opt the batched kernel into its dynamic shared memory once per device and
 // cache how many of its CTAs fit on the device at once.
-template <class S, class C, int K, bool PAIR>
+template <class S, class C, int K, int TY, bool PAIR>
 static cudaError_t batch_setup(int* occupancy) {
-  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
+  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, TY>;
   static unsigned long long done = 0;
   static int occ[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64) return cudaErrorInvalidDevice;
   if (!(done & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, 8, BATCH_PY, PAIR>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, TY, BATCH_PY, PAIR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, 8, BATCH_PY, PAIR>,
-                                                      256 / BATCH_PY, LY::SMEM);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, TY, BATCH_PY, PAIR>,
+                                                      batch_threads<TY, BATCH_PY, PAIR>(), LY::SMEM);
     if (e != cudaSuccess) return e;
     occ[dev] = nsm * (per > 0 ? per : 1);
     done |= 1ULL << dev;
@@ -189,15 +204,15 @@ static cudaError_t batch_setup(int* occupancy) {
   return cudaSuccess;
 }
 
-template <class S, class C, int K, bool PAIR>
+template <class S, class C, int K, int TY, bool PAIR>
 static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                                     const int* order, int nitems, int* queue, double* partials) {
-  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, 8>;
-  cudaError_t e = batch_setup<S, C, K, PAIR>(nullptr);
+  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, TY>;
+  cudaError_t e = batch_setup<S, C, K, TY, PAIR>(nullptr);
   if (e != cudaSuccess) return e;
-  const dim3 block = PAIR ? dim3(16, 8) : dim3(32, 8 / BATCH_PY);
-  k_stage_batch<S, C, K, 8, BATCH_PY, PAIR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
-                                                                            partials);
+  const dim3 block = PAIR ? dim3(16, 8) : dim3(32, TY / BATCH_PY);
+  k_stage_batch<S, C, K, TY, BATCH_PY, PAIR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
+                                                                             partials);
   return cudaGetLastError();
 }
 
@@ -205,13 +220,19 @@ template <class S, class C, int K>
 static cudaError_t launch_batch_kind(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                                      const int* order, int nitems, int* queue, double* partials, int* occupancy) {
   if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
+    if constexpr (is_rk4_kind(K)) {
+      if (batch_rk4_f32_rows() == 16) {
+        if (grid <= 0) return batch_setup<S, C, K, 16, true>(occupancy);
+        return launch_batch_one<S, C, K, 16, true>(grid, st, tab, items, order, nitems, queue, partials);
+      }
+    }
     if (batch_pair_layout()) {
-      if (grid <= 0) return batch_setup<S, C, K, true>(occupancy);
-      return launch_batch_one<S, C, K, true>(grid, st, tab, items, order, nitems, queue, partials);
+      if (grid <= 0) return batch_setup<S, C, K, 8, true>(occupancy);
+      return launch_batch_one<S, C, K, 8, true>(grid, st, tab, items, order, nitems, queue, partials);
     }
   }
-  if (grid <= 0) return batch_setup<S, C, K, false>(occupancy);
-  return launch_batch_one<S, C, K, false>(grid, st, tab, items, order, nitems, queue, partials);
+  if (grid <= 0) return batch_setup<S, C, K, 8, false>(occupancy);
+  return launch_batch_one<S, C, K, 8, false>(grid, st, tab, items, order, nitems, queue, partials);
 }
 
 template <class S, class C>
@@ -257,6 +278,11 @@ static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStr
                                      const StageArgs& a) {                                              \
     return launch_stage_tma_impl<S, C>(kind, R, ty, grid, st, m, a);                                    \
   }                                                                                                     \
+  int batch_rows_##TAG(int kind) {                                                                      \
+    return (std::is_same<S, float2>::value && std::is_same<C, float>::value && is_rk4_kind(kind))          \
+               ? batch_rk4_f32_rows()                                                                    \
+               : 8;                                                                                      \
+  }                                                                                                       \
   cudaError_t launch_batch_##TAG(int kind, int grid, cudaStream_t st, const BatchStage* tab,            \
                                  const BatchItem* items, const int* order, int nitems, int* queue,     \
                                  double* partials, int* occupancy) {                                   \

@@ -310,42 +310,49 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     if (okw) {
       const S* tile = (const S*)(rg.sring + sc_s * LY::ST_SLOT);
       const int gz = (k <= R || k >= g.nz - 1 - R) ? zghost_pos(k, g.nz, R, a.bcs, a.zghost) : NOGHOST;
-      Nb<C> n[PY];
+      // each row's neighbourhood is reduced to its Laplacian (and, with
+      // Urhs, x-derivative) right after its loads, so one row's neighbours
+      // are live at a time
+      cx<C> lap[PY], c0v[PY], dpx[PY];
       S pv[PY][NPW > 0 ? NPW : 1];
 #pragma unroll
       for (int r = 0; r < PY; ++r) {
         const int c0 = cofs[r];
-        n[r].c0 = to_c<C>(q[r][R]);
-        n[r].xm1 = to_c<C>(tile[c0 - 1]);
-        n[r].xp1 = to_c<C>(tile[c0 + 1]);
-        n[r].ym1 = to_c<C>(tile[c0 - TW]);
-        n[r].yp1 = to_c<C>(tile[c0 + TW]);
-        n[r].zm1 = to_c<C>(q[r][R - 1]);
-        n[r].zp1 = to_c<C>(q[r][R + 1]);
+        Nb<C> n;
+        n.c0 = to_c<C>(q[r][R]);
+        n.xm1 = to_c<C>(tile[c0 - 1]);
+        n.xp1 = to_c<C>(tile[c0 + 1]);
+        n.ym1 = to_c<C>(tile[c0 - TW]);
+        n.yp1 = to_c<C>(tile[c0 + TW]);
+        n.zm1 = to_c<C>(q[r][R - 1]);
+        n.zp1 = to_c<C>(q[r][R + 1]);
         if constexpr (R == 2) {
-          n[r].xm2 = to_c<C>(tile[c0 - 2]);
-          n[r].xp2 = to_c<C>(tile[c0 + 2]);
-          n[r].ym2 = to_c<C>(tile[c0 - 2 * TW]);
-          n[r].yp2 = to_c<C>(tile[c0 + 2 * TW]);
-          n[r].zm2 = to_c<C>(q[r][0]);
-          n[r].zp2 = to_c<C>(q[r][4]);
+          n.xm2 = to_c<C>(tile[c0 - 2]);
+          n.xp2 = to_c<C>(tile[c0 + 2]);
+          n.ym2 = to_c<C>(tile[c0 - 2 * TW]);
+          n.yp2 = to_c<C>(tile[c0 + 2 * TW]);
+          n.zm2 = to_c<C>(q[r][0]);
+          n.zp2 = to_c<C>(q[r][4]);
         } else {
-          n[r].xm2 = n[r].xp2 = n[r].ym2 = n[r].yp2 = n[r].zm2 = n[r].zp2 = cx<C>{0, 0};
+          n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
         }
+        lap[r] = site_lap<C, R>(a, n);
+        c0v[r] = n.c0;
+        dpx[r] = a.has_urhs ? site_dpx<C, R>(a, n) : cx<C>{0, 0};
         const int pofs = (tyt + r * TYT) * TX + tx;
 #pragma unroll
         for (int f = 0; f < NPW; ++f) pv[r][f] = pws[f * (TX * TY) + pofs];
       }
       constexpr int NPWX = NPW > 0 ? NPW : 1;
       if constexpr (KIND == K_ENERGY) {
-        sites_stage<S, C, R, KIND, PY, NPWX>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err);
+        sites_update<S, C, R, KIND, PY, NPWX>(a, lap, c0v, dpx, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err);
       } else {
         // the sites store their own values only; face ghosts are copied
         // after them, by tiles that touch an x/y face and on the first and
         // last R + 1 planes only (uniform branches, the site code stays one)
         S ns[PY];
-        sites_stage<S, C, R, KIND, PY, NPWX, false, false>(a, n, pv, act, i, jr, k, o, gz, cc, r_norm, r_en, r_err,
-                                                          ns);
+        sites_update<S, C, R, KIND, PY, NPWX, false, false>(a, lap, c0v, dpx, pv, act, i, jr, k, o, gz, cc, r_norm,
+                                                           r_en, r_err, ns);
         S* out = (S*)a.out;
         if (xyg) {
 #pragma unroll
@@ -719,24 +726,36 @@ struct BatchItem {
 // threads at FP32 (80 registers) and 4 at FP64 (+2-4 % on a batch of uneven
 // solves); Cash-Karp to 4 at FP32 (+8 % on a batch of RKF45 solves) and 3
 // at FP64 (neutral; stages 3-6 are held to 2 CTAs by shared memory anyway).
-template <class C, int KIND>
+// The complex64 pair layout on 32 x 16 items (four sites per thread) holds
+// twice the sites per thread and is fitted to 4 CTAs, as its single-solve
+// form.
+template <class C, int KIND, int TY = 8>
 __host__ __device__ constexpr int batch_min_blocks() {
-  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) ? (sizeof(C) == 4 ? 6 : 4)
-       : (KIND >= K_CK_1 && KIND <= K_CK_6)                                         ? (sizeof(C) == 4 ? 4 : 3)
-                                                                                     : 1;
+  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4)
+             ? (sizeof(C) == 4 ? (TY == 16 ? 4 : 6) : 4)
+         : (KIND >= K_CK_1 && KIND <= K_CK_6) ? (sizeof(C) == 4 ? 4 : 3)
+                                              : 1;
+}
+
+// Threads of a batched CTA: 32 x TY/PY, or with the pair layout 16 x 8 (one
+// row per thread on 32 x 8 items, two rows on 32 x 16 items).
+template <int TY, int PY, bool PAIR>
+__host__ __device__ constexpr int batch_threads() {
+  return PAIR ? 128 : 32 * TY / PY;
 }
 
 // PAIR (complex64 storage with the FP32 stencil only): 16 x 8 threads, each
-// with two x-adjacent sites of one row of the 32 x 8 item tile
+// with two x-adjacent sites in TY/8 rows of the 32 x TY item tile
 // (tma_item_pair); otherwise 32 x TY/PY threads with PY rows each.
 template <class S, class C, int KIND, int TY, int PY, bool PAIR = false>
-__global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k_stage_batch(const BatchStage* __restrict__ tab,
-                                                         const BatchItem* __restrict__ items,
-                                                         const int* __restrict__ order, int nitems,
-                                                         int* queue, double* partials) {
-  static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && 32 * TY / PY == 16 * TY),
-                "the pair layout is for complex64 / FP32 with one row per thread");
+__global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_blocks<C, KIND, PAIR ? TY : 8>()))
+    k_stage_batch(const BatchStage* __restrict__ tab, const BatchItem* __restrict__ items,
+                  const int* __restrict__ order, int nitems, int* queue, double* partials) {
+  static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && (TY == 8 || TY == 16)),
+                "the pair layout is for complex64 / FP32 on 32 x 8 or 32 x 16 items");
+  constexpr int PYP = TY / 8;  // rows per thread of the pair layout
   using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
+  constexpr int NT = batch_threads<TY, PY, PAIR>();
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
   __shared__ int s_w[2];  // item taken from the queue, double-buffered by turn parity
@@ -767,11 +786,11 @@ __global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k
     bool ok;
     if constexpr (PAIR) {
       if (R == 1)
-        ok = tma_item_pair<C, 1, KIND, TY, 1, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                  r_err);
+        ok = tma_item_pair<C, 1, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                    r_err);
       else
-        ok = tma_item_pair<C, 2, KIND, TY, 1, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                  r_err);
+        ok = tma_item_pair<C, 2, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                    r_err);
     } else {
       if (R == 1)
         ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
@@ -781,7 +800,7 @@ __global__ void __launch_bounds__(32 * TY / PY, (batch_min_blocks<C, KIND>())) k
                                                  r_err);
     }
     if (!ok) return;
-    if (partials) block_reduce_store_at<32 * TY / PY>(r_norm, r_en, r_err, partials, w);
+    if (partials) block_reduce_store_at<NT>(r_norm, r_en, r_err, partials, w);
   }
 }
 
