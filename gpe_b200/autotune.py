@@ -40,13 +40,16 @@ def save_cache(c: dict) -> None:
 
 def time_rk4(rp: RunParams, steps: int = 20, target_sites: int = 32 << 20) -> float:
     """Seconds per site per RK4 step when the GPU is kept busy with copies of
-    this solve in one pool (the batched setting the tuned shape is used in)."""
+    this solve in one pool (the batched setting the tuned shape is used in).
+    The copies add up to target_sites for every size, so small grids are
+    timed on a saturated GPU as they run in a mixed batch, not on a
+    half-empty one where many short items win."""
     import time
 
     from .pool import Pool
 
     n_sites = rp.nx * rp.ny * rp.nz
-    copies = max(1, min(64, -(-target_sites // n_sites)))
+    copies = max(1, -(-target_sites // n_sites))
     pool = Pool(Pool.solve_bytes(rp) * copies + (64 << 20))
     psi = np.ones((rp.nz, rp.ny, rp.nx), np.complex64 if rp.storage == "c64" else np.complex128)
     for c in range(copies):

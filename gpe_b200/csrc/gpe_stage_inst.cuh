@@ -164,12 +164,14 @@ inline bool batch_pair_layout() {
 }
 
 // Item rows of the batched RK4 kernels for complex64 storage with the FP32
-// stencil: 32 x 16 items with the pair layout (two rows per thread), unless
-// GPE_BATCH_ROWS=8.  Every other class uses 32 x 8 items.
+// stencil: 32 x 8 items (one row of x pairs per thread); GPE_BATCH_ROWS=16
+// selects 32 x 16 items with two rows per thread (no faster on an uneven
+// mix of 32^3-160^3 solves: 40.1 against 40.5 G site-updates/s).  Every
+// other class uses 32 x 8 items.
 inline int batch_rk4_f32_rows() {
   static const int rows = [] {
     const char* e = getenv("GPE_BATCH_ROWS");
-    return (e && atoi(e) == 8) || !batch_pair_layout() ? 8 : 16;
+    return (e && atoi(e) == 16) && batch_pair_layout() ? 16 : 8;
   }();
   return rows;
 }
