@@ -168,16 +168,6 @@ inline bool batch_pair_layout() {
 // selects 32 x 16 items with two rows per thread (no faster on an uneven
 // mix of 32^3-160^3 solves: 40.1 against 40.5 G site-updates/s).  Every
 // other class uses 32 x 8 items.
-// Alternate the z-march direction of a solve's z-chunks in batched launches
-// (GPE_BATCH_ZALT=0 marches every chunk upward).
-inline int batch_zalt() {
-  static const int on = [] {
-    const char* e = getenv("GPE_BATCH_ZALT");
-    return (e && atoi(e) == 0) ? 0 : 1;
-  }();
-  return on;
-}
-
 inline int batch_rk4_f32_rows() {
   static const int rows = [] {
     const char* e = getenv("GPE_BATCH_ROWS");
@@ -224,7 +214,7 @@ static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage*
   if (e != cudaSuccess) return e;
   const dim3 block = PAIR ? dim3(16, 8) : dim3(32, TY / BATCH_PY);
   k_stage_batch<S, C, K, TY, BATCH_PY, PAIR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
-                                                                             partials, batch_zalt());
+                                                                             partials);
   return cudaGetLastError();
 }
 

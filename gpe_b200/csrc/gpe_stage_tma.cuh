@@ -176,12 +176,10 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
 // One work item: the 32 x TY tile (bx, by) of planes [bz*zc, bz*zc+zc) of one
 // solve, processed by 32 x (TY/PY) threads, each owning PY rows of the tile
 // (rows ty, ty + TY/PY, ...) so that the per-plane waits, barrier and ring
-// bookkeeping are shared by PY sites.  DOWN marches the chunk from its top
-// plane down (the z queue then holds planes k+R .. k-R); the per-site
-// arithmetic is the same, so results are bitwise those of the upward march.
-// Returns false when a bounded wait expired (the caller must stop; the
-// copies this item issued have been drained and a.status set).
-template <class S, class C, int R, int KIND, int TY, int PY, class LY, bool DOWN = false>
+// bookkeeping are shared by PY sites.  Returns false when a bounded wait
+// expired (the caller must stop; the copies this item issued have been
+// drained and a.status set).
+template <class S, class C, int R, int KIND, int TY, int PY, class LY>
 __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                          TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                          double& r_err) {
@@ -210,7 +208,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   auto issue_stencil = [&](int l) {
     const int G = SB + l, s = G % NSS;
     mbar_arrive_expect_tx(&rg.sbar[s], ST_BYTES);
-    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, (DOWN ? ke - 1 + R - l : kb - R + l) + 2);
+    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, kb - R + l + 2);
     issued_s = l + 1;
   };
   auto issue_pw = [&](int m) {
@@ -219,7 +217,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
       mbar_arrive_expect_tx(&rg.pbar[s], NPW * PW1);
 #pragma unroll
       for (int f = 0; f < NPW; ++f)
-        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, (DOWN ? ke - 1 - m : kb + m) + 2);
+        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, kb + m + 2);
       issued_p = m + 1;
     }
   };
@@ -252,7 +250,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     jr[r] = by * TY + ty;
     act[r] = (i < g.nx) && (jr[r] < g.ny);
     cofs[r] = (ty + R) * TW + tx + HX;
-    o[r] = (long long)((DOWN ? ke - 1 : kb) + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i;
+    o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i;
     cc[r] = column_consts<C>(a, i, jr[r], R, act[r]);
   }
   // does this tile hold a site with an x or y ghost?  Ghosts come from the
@@ -294,7 +292,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
 
   for (int m = 0; m < M; ++m) {
-    const int k = DOWN ? ke - 1 - m : kb + m;
+    const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
     bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
     {
@@ -326,15 +324,15 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
         n.xp1 = to_c<C>(tile[c0 + 1]);
         n.ym1 = to_c<C>(tile[c0 - TW]);
         n.yp1 = to_c<C>(tile[c0 + TW]);
-        n.zm1 = to_c<C>(q[r][DOWN ? R + 1 : R - 1]);
-        n.zp1 = to_c<C>(q[r][DOWN ? R - 1 : R + 1]);
+        n.zm1 = to_c<C>(q[r][R - 1]);
+        n.zp1 = to_c<C>(q[r][R + 1]);
         if constexpr (R == 2) {
           n.xm2 = to_c<C>(tile[c0 - 2]);
           n.xp2 = to_c<C>(tile[c0 + 2]);
           n.ym2 = to_c<C>(tile[c0 - 2 * TW]);
           n.yp2 = to_c<C>(tile[c0 + 2 * TW]);
-          n.zm2 = to_c<C>(q[r][DOWN ? 4 : 0]);
-          n.zp2 = to_c<C>(q[r][DOWN ? 0 : 4]);
+          n.zm2 = to_c<C>(q[r][0]);
+          n.zp2 = to_c<C>(q[r][4]);
         } else {
           n.xm2 = n.xp2 = n.ym2 = n.yp2 = n.zm2 = n.zp2 = cx<C>{0, 0};
         }
@@ -376,7 +374,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
     for (int r = 0; r < PY; ++r) {
 #pragma unroll
       for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
-      o[r] += DOWN ? -g.pz : g.pz;
+      o[r] += g.pz;
     }
     if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
     if (++sc_s == NSS) sc_s = 0;
@@ -434,7 +432,7 @@ __device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool ac
     *p = v0;
 }
 
-template <class C, int R, int KIND, int TY, int PY, class LY, bool DOWN = false>
+template <class C, int R, int KIND, int TY, int PY, class LY>
 __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                               TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                               double& r_err) {
@@ -465,7 +463,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
   auto issue_stencil = [&](int l) {
     const int G = SB + l, s = G % NSS;
     mbar_arrive_expect_tx(&rg.sbar[s], ST_BYTES);
-    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, (DOWN ? ke - 1 + R - l : kb - R + l) + 2);
+    tma_load_3d(rg.sring + s * LY::ST_SLOT, &maps.in, &rg.sbar[s], cxs, cys, kb - R + l + 2);
     issued_s = l + 1;
   };
   auto issue_pw = [&](int m) {
@@ -474,7 +472,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
       mbar_arrive_expect_tx(&rg.pbar[s], NPW * PW1);
 #pragma unroll
       for (int f = 0; f < NPW; ++f)
-        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, (DOWN ? ke - 1 - m : kb + m) + 2);
+        tma_load_3d(rg.pring + s * LY::PW_SLOT + f * PW1, &maps.pw[f], &rg.pbar[s], cxp, cyp, kb + m + 2);
       issued_p = m + 1;
     }
   };
@@ -504,7 +502,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     jr[r] = by * TY + ty;
     cofs[r] = (ty + R) * TW + 2 * tx + HX;
     pofs[r] = ty * TX + 2 * tx;
-    o[r] = (long long)((DOWN ? ke - 1 : kb) + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i0;
+    o[r] = (long long)(kb + 2) * g.pz + (long long)(jr[r] + 2) * g.px + g.xoff + i0;
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int q = 2 * r + s;
@@ -545,7 +543,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
   int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
 
   for (int m = 0; m < M; ++m) {
-    const int k = DOWN ? ke - 1 - m : kb + m;
+    const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
     bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
     {
@@ -585,10 +583,10 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
         n1.ym1 = to_c<C>(hi2(ym1));
         n0.yp1 = to_c<C>(lo2(yp1));
         n1.yp1 = to_c<C>(hi2(yp1));
-        n0.zm1 = to_c<C>(lo2(q[r][DOWN ? R + 1 : R - 1]));
-        n1.zm1 = to_c<C>(hi2(q[r][DOWN ? R + 1 : R - 1]));
-        n0.zp1 = to_c<C>(lo2(q[r][DOWN ? R - 1 : R + 1]));
-        n1.zp1 = to_c<C>(hi2(q[r][DOWN ? R - 1 : R + 1]));
+        n0.zm1 = to_c<C>(lo2(q[r][R - 1]));
+        n1.zm1 = to_c<C>(hi2(q[r][R - 1]));
+        n0.zp1 = to_c<C>(lo2(q[r][R + 1]));
+        n1.zp1 = to_c<C>(hi2(q[r][R + 1]));
         if constexpr (R == 2) {
           const float4 ym2 = lds_pair(c - 2 * TW), yp2 = lds_pair(c + 2 * TW);
           n0.xm2 = to_c<C>(lo2(xl));
@@ -599,10 +597,10 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
           n1.ym2 = to_c<C>(hi2(ym2));
           n0.yp2 = to_c<C>(lo2(yp2));
           n1.yp2 = to_c<C>(hi2(yp2));
-          n0.zm2 = to_c<C>(lo2(q[r][DOWN ? 4 : 0]));
-          n1.zm2 = to_c<C>(hi2(q[r][DOWN ? 4 : 0]));
-          n0.zp2 = to_c<C>(lo2(q[r][DOWN ? 0 : 4]));
-          n1.zp2 = to_c<C>(hi2(q[r][DOWN ? 0 : 4]));
+          n0.zm2 = to_c<C>(lo2(q[r][0]));
+          n1.zm2 = to_c<C>(hi2(q[r][0]));
+          n0.zp2 = to_c<C>(lo2(q[r][4]));
+          n1.zp2 = to_c<C>(hi2(q[r][4]));
         } else {
           n0.xm2 = n0.xp2 = n0.ym2 = n0.yp2 = n0.zm2 = n0.zp2 = cx<C>{0, 0};
           n1.xm2 = n1.xp2 = n1.ym2 = n1.yp2 = n1.zm2 = n1.zp2 = cx<C>{0, 0};
@@ -662,7 +660,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     for (int r = 0; r < PY; ++r) {
 #pragma unroll
       for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
-      o[r] += DOWN ? -g.pz : g.pz;
+      o[r] += g.pz;
     }
     if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
     if (++sc_s == NSS) sc_s = 0;
@@ -752,7 +750,7 @@ __host__ __device__ constexpr int batch_threads() {
 template <class S, class C, int KIND, int TY, int PY, bool PAIR = false>
 __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_blocks<C, KIND, PAIR ? TY : 8>()))
     k_stage_batch(const BatchStage* __restrict__ tab, const BatchItem* __restrict__ items,
-                  const int* __restrict__ order, int nitems, int* queue, double* partials, int zalt) {
+                  const int* __restrict__ order, int nitems, int* queue, double* partials) {
   static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && (TY == 8 || TY == 16)),
                 "the pair layout is for complex64 / FP32 on 32 x 8 or 32 x 16 items");
   constexpr int PYP = TY / 8;  // rows per thread of the pair layout
@@ -786,32 +784,20 @@ __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_bloc
     const int R = sa.R;
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;
-    // with zalt, odd z-chunks march downward: two neighbouring chunks then
-    // read the halo planes they share at the same time (both at their start
-    // or both at their end), so the second read finds them in L2
-    const bool down = zalt && (it.bz & 1);
     if constexpr (PAIR) {
       if (R == 1)
-        ok = down ? tma_item_pair<C, 1, KIND, TY, PYP, LY, true>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort,
-                                                                 r_norm, r_en, r_err)
-                  : tma_item_pair<C, 1, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
-                                                           r_en, r_err);
+        ok = tma_item_pair<C, 1, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                    r_err);
       else
-        ok = down ? tma_item_pair<C, 2, KIND, TY, PYP, LY, true>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort,
-                                                                 r_norm, r_en, r_err)
-                  : tma_item_pair<C, 2, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
-                                                           r_en, r_err);
+        ok = tma_item_pair<C, 2, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                    r_err);
     } else {
       if (R == 1)
-        ok = down ? tma_item<S, C, 1, KIND, TY, PY, LY, true>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort,
-                                                              r_norm, r_en, r_err)
-                  : tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
-                                                        r_en, r_err);
+        ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                 r_err);
       else
-        ok = down ? tma_item<S, C, 2, KIND, TY, PY, LY, true>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort,
-                                                              r_norm, r_en, r_err)
-                  : tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
-                                                        r_en, r_err);
+        ok = tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                 r_err);
     }
     if (!ok) return;
     if (partials) block_reduce_store_at<NT>(r_norm, r_en, r_err, partials, w);
