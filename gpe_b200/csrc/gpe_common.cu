@@ -182,6 +182,7 @@ StageArgs make_base_args(const gpe_params& p, const Geom& g, int R, int zc, cons
   a.zc = zc;
   a.has_urhs = (p.Urhs != 0.0) && p.eqn != 4;
   a.has_diss = (p.diss_amp != 0.0) && (p.eqn == 1 || p.eqn == 3);
+  a.eqn4_plain = p.eqn == 4 && p.omx == 0.0 && p.omy == 0.0 && p.omz == 0.0 && p.gamma == 0.0;
   const double dx2 = d[0] * d[0], dy2 = d[1] * d[1], dz2 = d[2] * d[2];
   if (p.order == 2) {
     a.ixx = 1.0 / dx2;

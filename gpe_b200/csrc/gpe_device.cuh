@@ -94,6 +94,7 @@ struct alignas(16) StageArgs {
   double* partials;             // [nblocks][RED_SLOTS]
   int* status;                  // device status word: non-zero = a bounded wait expired
   int zghost;                   // z ghosts the producer writes: bit 0 below the grid, bit 1 above
+  int eqn4_plain;               // eqn 4 with V = 0 and gamma = 0 (the trap and damping terms vanish)
 };
 
 static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is copied in 16-byte words");
@@ -337,9 +338,21 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
     // FP64 as 0.5 ((vx + vy) + vz); in FP32 compute as the sum of the
     // column's and the plane's halves, each rounded once to float (no FP64
     // operations or conversions per site)
+    const C g = (C)a.g_nl, mu = (C)a.mu, gm = (C)a.gamma;
+    if (a.eqn4_plain) {
+      // V = 0, gamma = 0: the same sums without their zero terms (the
+      // results agree bit for bit up to the sign of a zero)
+#pragma unroll
+      for (int q = 0; q < PY; ++q) {
+        const C wr = (-(C)0.5 * lap[q].r + g * (n2[q] * p[q].r)) - mu * p[q].r;
+        const C wi = (-(C)0.5 * lap[q].i + g * (n2[q] * p[q].i)) - mu * p[q].i;
+        r[q].r = wi;
+        r[q].i = -wr;
+      }
+      return;
+    }
     const double vz = a.vz[k];
     const float vzh = (float)(0.5 * vz);
-    const C g = (C)a.g_nl, mu = (C)a.mu, gm = (C)a.gamma;
 #pragma unroll
     for (int q = 0; q < PY; ++q) {
       C v;
