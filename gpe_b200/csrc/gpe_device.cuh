@@ -386,11 +386,12 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
     for (int q = 0; q < PY; ++q) dd[q] = 0;
     if (a.has_diss) {
       const double sz = a.sz[k];
-#pragma unroll
       if constexpr (sizeof(C) == sizeof(double)) {
+#pragma unroll
         for (int q = 0; q < PY; ++q) dd[q] = 0.5 * (a.diss_amp * (cc[q].sxy + sz));
       } else {
         const C amp = (C)a.diss_amp, szf = (C)sz;
+#pragma unroll
         for (int q = 0; q < PY; ++q) dd[q] = (C)0.5 * (amp * (cc[q].sxy + szf));
       }
     }
