@@ -322,9 +322,10 @@ def c4_mix(storage: str = "c64", tuned: bool = True):
     """The 64 uneven solves of the batched workload: cubic sizes uniform in
     {32, 48, ..., 160}, periodic/reflective and 2nd/4th order mixed (seeded),
     RK4 dt = 0.01, eqn 4, ring (r0 in [2,6]) / random-phase (cutoff in
-    [1,2]) initial states alternating.  tuned: tile_zc per size from the
-    autotuner (measured on a cache miss), else the pool's default.  Returns
-    [(params, page-locked input, page-locked result buffer)] and the cache."""
+    [1,2]) initial states alternating.  tuned: tile_zc = min(cap, n) with
+    the z-chunk cap the autotuner picks for this batch (measured on a cache
+    miss), else the pool's default.  Returns [(params, page-locked input,
+    page-locked result buffer)] and the cache."""
     from gpe_b200 import _lib as L
     from gpe_b200 import autotune
     from gpe_b200 import ic
@@ -340,21 +341,22 @@ def c4_mix(storage: str = "c64", tuned: bool = True):
         r0, kc = float(rng.uniform(2, 6)), float(rng.uniform(1, 2))
         h = 0.25 * (n - 1)
         rp = RunParams(nx=n, ny=n, nz=n, xr=h, yr=h, zr=h, tau=0.01, scheme="rk4", eqn_to_solve=4, bcs=bcs,
-                       order=order, g=1.0, mu=1.0, storage=storage,
-                       tile_zc=autotune.best_zc(n, order, storage, cache) if tuned else 0)
+                       order=order, g=1.0, mu=1.0, storage=storage)
         psi = ic.vortex_ring(rp, "xy", r0=r0) if k % 2 == 0 else ic.random_phase(rp, seed=k, kc=kc)
         # the caller's input and result buffers: page-locked, allocated once
         host = L.pinned_empty(psi.shape, dt)
         host[...] = psi
         solves.append((rp, host, L.pinned_empty(psi.shape, dt)))
     if tuned:
+        cap = autotune.tune_mix([s[0] for s in solves], [s[1] for s in solves], cache)
+        solves = [(rp.replace(tile_zc=min(cap, rp.nz)), a, b) for rp, a, b in solves]
         autotune.save_cache(cache)
     return solves, cache
 
 
 def batched_leg(args, torch):
     """The c4_mix solves in one pool, complex64 storage with FP64
-    reductions, 500 steps, tile_zc per size from the autotuner.  Timed on the
+    reductions, 500 steps, the z-chunk cap from the autotuner.  Timed on the
     host clock from the first submission to the last retired result (state
     upload and download included); latencies are per solve, all submitted at
     t = 0."""
@@ -394,7 +396,7 @@ def batched_leg(args, torch):
             "steps": C4_STEPS, "wall_s": wall, "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "storage": "c64",
             "stepping_rate": sites * C4_SHORT / resident,
-            "tile_zc": {k: v["zc"] for k, v in cache.items()},
+            "tile_zc": {f"n{rp.nx}": rp.tile_zc for rp, _, _ in solves},
             "timing": "value: host clock, first submit to last result, uploads/downloads included (the caller's "
                       "states and result buffers in page-locked host memory); stepping_rate: host clock around "
                       f"{C4_SHORT} steps of the whole mix resident on the device (synchronised both sides)"}

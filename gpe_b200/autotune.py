@@ -1,7 +1,9 @@
-"""Tile-shape autotuner: for each (grid size, FD order, storage) pick the
-number of z planes per CTA work item (tile_zc) that gives the fastest RK4
-step, by timing candidates on the GPU; results are cached in a JSON file so
-a size is measured once per machine.
+"""Tile-shape autotuner: pick the number of z planes per CTA work item
+(tile_zc) that gives the fastest RK4 step, by timing candidates on the GPU,
+either per (grid size, FD order, storage) in a pool of copies of one solve
+(best_zc) or for a given batch of uneven solves as a whole (tune_mix: one
+cap on the z-chunk length for all of them).  Results are cached in a JSON
+file so a size or a mix is measured once per machine.
 
 The x-y tile is fixed by the TMA box (32 x 8 sites); tile_zc trades the
 z-halo re-read (2R planes per item) against the number of items, which
@@ -87,3 +89,48 @@ def tune(sizes, orders=(2, 4), storages=("c64",)) -> dict:
                 best_zc(n, o, st, cache)
     save_cache(cache)
     return cache
+
+
+MIX_CAPS = (32, 48, 64, 96)
+
+
+def _mix_key(params) -> str:
+    import hashlib
+
+    sig = sorted((p.nx, p.ny, p.nz, p.order, p.bcs, p.storage, p.scheme) for p in params)
+    return "mix_" + hashlib.sha1(repr(sig).encode()).hexdigest()[:16]
+
+
+def time_mix(params, states, cap: int, steps: int = 20) -> float:
+    """Seconds per RK4 step of the whole batch with tile_zc = min(cap, nz)."""
+    import time
+
+    from .pool import Pool
+
+    runs = [p.replace(tile_zc=min(cap, p.nz)) for p in params]
+    pool = Pool(sum(Pool.solve_bytes(p) for p in runs) + (256 << 20))
+    for k, (p, psi) in enumerate(zip(runs, states)):
+        assert pool.submit(p, psi, steps + 4, k)
+    pool.step(3)  # joins the batch, captures the step graph
+    t0 = time.perf_counter()
+    pool.step(steps)
+    t = time.perf_counter() - t0
+    pool.run_all()
+    pool.close()
+    return t / steps
+
+
+def tune_mix(params, states, cache: dict | None = None) -> int:
+    """The z-chunk cap that steps this batch of solves fastest (measured on a
+    cache miss): each solve then uses tile_zc = min(cap, nz).  A cap suits
+    an uneven batch better than per-size choices timed in homogeneous pools:
+    the other solves keep the GPU busy, so items can be long."""
+    own = cache is None
+    cache = load_cache() if cache is None else cache
+    k = _mix_key(params)
+    if k not in cache:
+        times = {cap: time_mix(params, states, cap) for cap in MIX_CAPS}
+        cache[k] = {"cap": min(times, key=times.get), "s_per_step": times}
+        if own:
+            save_cache(cache)
+    return int(cache[k]["cap"])
