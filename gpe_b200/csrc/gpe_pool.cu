@@ -28,11 +28,11 @@
 #include "gpe_ic.h"
 
 namespace gpe {
-cudaError_t launch_batch_f64(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+cudaError_t launch_batch_f64(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                              const int* order, int nitems, int* queue, double* partials, int* occupancy);
-cudaError_t launch_batch_f32(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+cudaError_t launch_batch_f32(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                              const int* order, int nitems, int* queue, double* partials, int* occupancy);
-cudaError_t launch_batch_f32x(int kind, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+cudaError_t launch_batch_f32x(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                               const int* order, int nitems, int* queue, double* partials, int* occupancy);
 int batch_rows_f64(int kind);
 int batch_rows_f32(int kind);
@@ -44,6 +44,13 @@ using namespace gpe;
 namespace {
 
 enum { CM_F64 = 0, CM_F32 = 1, CM_F32X = 2, NCM = 3 };
+// Classes of solves that share launches: (precision mode, stencil radius) x
+// scheme family.  Solves of the two FD orders run in separate classes, so
+// each batched kernel carries one item body and rings sized for its radius.
+constexpr int NCLS = NCM * 2;
+inline int class_of(int cmode, int R) { return cmode * 2 + (R - 1); }
+inline int class_cmode(int cls) { return cls / 2; }
+inline int class_radius(int cls) { return cls % 2 + 1; }
 enum { FAM_RK4 = 0, FAM_RK45 = 1, NFAM = 2 };
 
 // First-fit allocator over [0, total) with coalescing; 256-byte granules.
@@ -207,7 +214,7 @@ struct gpe_pool {
   Arena alloc;
   int* d_status = nullptr;
   std::vector<Solve*> pending;
-  Class cls[NCM][NFAM];
+  Class cls[NCLS][NFAM];
   std::deque<gpe_result> done;
   std::string err;
   std::chrono::steady_clock::time_point t0;
@@ -232,13 +239,14 @@ int cmode_of(const gpe_params& p) {
   return p.compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32;
 }
 
-cudaError_t launch_batch(int cmode, int kind, int grid, cudaStream_t st, const BatchStage* tab,
+cudaError_t launch_batch(int cls, int kind, int grid, cudaStream_t st, const BatchStage* tab,
                          const BatchItem* items, const int* order, int nitems, int* queue, double* partials,
                          int* occ) {
-  switch (cmode) {
-    case CM_F64: return launch_batch_f64(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
-    case CM_F32: return launch_batch_f32(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
-    default: return launch_batch_f32x(kind, grid, st, tab, items, order, nitems, queue, partials, occ);
+  const int R = class_radius(cls);
+  switch (class_cmode(cls)) {
+    case CM_F64: return launch_batch_f64(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
+    case CM_F32: return launch_batch_f32(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
+    default: return launch_batch_f32x(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
   }
 }
 
@@ -252,9 +260,9 @@ int batch_rows(int cmode, int fam) {
   }
 }
 
-int grid_for(int cmode, int kind, int nitems) {
+int grid_for(int cls, int kind, int nitems) {
   int occ = 0;
-  launch_batch(cmode, kind, 0, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, &occ);
+  launch_batch(cls, kind, 0, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, &occ);
   return std::max(1, std::min(nitems, occ));
 }
 
@@ -738,15 +746,15 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
   // continuous batching: solves submitted since the last step join now
   for (Solve* s : P->pending) {
     s->t_start = now_s(P->t0);
-    Class& c = P->cls[s->cmode][s->fam];
+    Class& c = P->cls[class_of(s->cmode, s->R)][s->fam];
     c.solves.push_back(s);
     c.dirty = true;
   }
   P->pending.clear();
   // RK4 classes: enqueue their chunk on their own streams and let them run
   // while the RKF45 classes go through their attempts
-  int64_t chunks[NCM] = {0};
-  for (int cm = 0; cm < NCM; ++cm) {
+  int64_t chunks[NCLS] = {0};
+  for (int cm = 0; cm < NCLS; ++cm) {
     Class& c = P->cls[cm][FAM_RK4];
     int64_t chunk = max_steps;
     for (Solve* s : c.solves) chunk = std::min(chunk, s->nsteps - s->done);
@@ -755,25 +763,25 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
       chunks[cm] = chunk;
     }
   }
-  for (int cm = 0; cm < NCM; ++cm)
+  for (int cm = 0; cm < NCLS; ++cm)
     for (Solve* s : P->cls[cm][FAM_RK45].solves) {
       s->quota = std::min(max_steps, s->nsteps - s->done);
       s->dte_r = s->dr;
       s->dte_i = s->di;
     }
   for (int round = 0; round < 1000000; ++round) {
-    std::vector<Solve*> sv[NCM];
+    std::vector<Solve*> sv[NCLS];
     bool any = false;
-    for (int cm = 0; cm < NCM; ++cm) {
+    for (int cm = 0; cm < NCLS; ++cm) {
       if (int rc = rk45_enqueue(P, cm, sv[cm])) return rc;
       any |= !sv[cm].empty();
     }
     if (!any) break;
-    for (int cm = 0; cm < NCM; ++cm)
+    for (int cm = 0; cm < NCLS; ++cm)
       if (!sv[cm].empty())
         if (int rc = rk45_collect(P, cm, sv[cm])) return rc;
   }
-  for (int cm = 0; cm < NCM; ++cm)
+  for (int cm = 0; cm < NCLS; ++cm)
     if (chunks[cm])
       if (int rc = rk4_collect(P, cm, chunks[cm])) return rc;
   // a stage kernel whose bounded waits expired left the status word set: the
@@ -782,14 +790,14 @@ int gpe_pool_step(gpe_pool* P, int64_t max_steps, int32_t* n_active) {
   // the error; the pool itself stays usable
   const int timeout_rc = check_status(P);
   if (timeout_rc == GPE_ERR_TIMEOUT)
-    for (int cm = 0; cm < NCM; ++cm)
+    for (int cm = 0; cm < NCLS; ++cm)
       for (int fam = 0; fam < NFAM; ++fam)
         for (Solve* s : P->cls[cm][fam].solves) s->status = GPE_ERR_TIMEOUT;
   else if (timeout_rc)
     return timeout_rc;
   // retire finished solves
   int active = 0;
-  for (int cm = 0; cm < NCM; ++cm)
+  for (int cm = 0; cm < NCLS; ++cm)
     for (int fam = 0; fam < NFAM; ++fam) {
       Class& c = P->cls[cm][fam];
       std::vector<Solve*> keep, fin;
@@ -875,7 +883,7 @@ void gpe_pool_destroy(gpe_pool* P) {
   cudaSetDevice(P->dev);
   if (P->st) cudaStreamSynchronize(P->st);
   for (Solve* s : P->pending) delete s;
-  for (int cm = 0; cm < NCM; ++cm)
+  for (int cm = 0; cm < NCLS; ++cm)
     for (int fam = 0; fam < NFAM; ++fam) {
       Class& c = P->cls[cm][fam];
       for (Solve* s : c.solves) delete s;

@@ -182,21 +182,21 @@ __host__ __device__ constexpr bool is_rk4_kind(int k) {
 
 // Opt the batched kernel into its dynamic shared memory once per device and
 // cache how many of its CTAs fit on the device at once.
-template <class S, class C, int K, int TY, bool PAIR>
+template <class S, class C, int K, int TY, bool PAIR, int RR>
 static cudaError_t batch_setup(int* occupancy) {
-  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, TY>;
+  using LY = TmaLayout<S, RR, StageTraits<K>::NPW, TY>;
   static unsigned long long done = 0;
   static int occ[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64) return cudaErrorInvalidDevice;
   if (!(done & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, TY, BATCH_PY, PAIR>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, TY, BATCH_PY, PAIR>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR>,
                                                       batch_threads<TY, BATCH_PY, PAIR>(), LY::SMEM);
     if (e != cudaSuccess) return e;
     occ[dev] = nsm * (per > 0 ? per : 1);
@@ -206,45 +206,55 @@ static cudaError_t batch_setup(int* occupancy) {
   return cudaSuccess;
 }
 
-template <class S, class C, int K, int TY, bool PAIR>
+template <class S, class C, int K, int TY, bool PAIR, int RR>
 static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
                                     const int* order, int nitems, int* queue, double* partials) {
-  using LY = TmaLayout<S, 2, StageTraits<K>::NPW, TY>;
-  cudaError_t e = batch_setup<S, C, K, TY, PAIR>(nullptr);
+  using LY = TmaLayout<S, RR, StageTraits<K>::NPW, TY>;
+  cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR>(nullptr);
   if (e != cudaSuccess) return e;
   const dim3 block = PAIR ? dim3(16, 8) : dim3(32, TY / BATCH_PY);
-  k_stage_batch<S, C, K, TY, BATCH_PY, PAIR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
-                                                                             partials);
+  k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
+                                                                                 partials);
   return cudaGetLastError();
 }
 
-template <class S, class C, int K>
-static cudaError_t launch_batch_kind(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                                     const int* order, int nitems, int* queue, double* partials, int* occupancy) {
+template <class S, class C, int K, int RR>
+static cudaError_t launch_batch_kind_r(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
+                                       const int* order, int nitems, int* queue, double* partials,
+                                       int* occupancy) {
   if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
     if constexpr (is_rk4_kind(K)) {
       if (batch_rk4_f32_rows() == 16) {
-        if (grid <= 0) return batch_setup<S, C, K, 16, true>(occupancy);
-        return launch_batch_one<S, C, K, 16, true>(grid, st, tab, items, order, nitems, queue, partials);
+        if (grid <= 0) return batch_setup<S, C, K, 16, true, RR>(occupancy);
+        return launch_batch_one<S, C, K, 16, true, RR>(grid, st, tab, items, order, nitems, queue, partials);
       }
     }
     if (batch_pair_layout()) {
-      if (grid <= 0) return batch_setup<S, C, K, 8, true>(occupancy);
-      return launch_batch_one<S, C, K, 8, true>(grid, st, tab, items, order, nitems, queue, partials);
+      if (grid <= 0) return batch_setup<S, C, K, 8, true, RR>(occupancy);
+      return launch_batch_one<S, C, K, 8, true, RR>(grid, st, tab, items, order, nitems, queue, partials);
     }
   }
-  if (grid <= 0) return batch_setup<S, C, K, 8, false>(occupancy);
-  return launch_batch_one<S, C, K, 8, false>(grid, st, tab, items, order, nitems, queue, partials);
+  if (grid <= 0) return batch_setup<S, C, K, 8, false, RR>(occupancy);
+  return launch_batch_one<S, C, K, 8, false, RR>(grid, st, tab, items, order, nitems, queue, partials);
+}
+
+template <class S, class C, int K>
+static cudaError_t launch_batch_kind(int R, int grid, cudaStream_t st, const BatchStage* tab,
+                                     const BatchItem* items, const int* order, int nitems, int* queue,
+                                     double* partials, int* occupancy) {
+  if (R == 1) return launch_batch_kind_r<S, C, K, 1>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
+  if (R == 2) return launch_batch_kind_r<S, C, K, 2>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
+  return cudaErrorInvalidValue;
 }
 
 template <class S, class C>
-static cudaError_t launch_batch_impl(int kind, int grid, cudaStream_t st, const BatchStage* tab,
+static cudaError_t launch_batch_impl(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab,
                                      const BatchItem* items, const int* order, int nitems, int* queue,
                                      double* partials, int* occupancy) {
   switch (kind) {
 #define GPE_BCASE(K) \
   case K:            \
-    return launch_batch_kind<S, C, K>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
+    return launch_batch_kind<S, C, K>(R, grid, st, tab, items, order, nitems, queue, partials, occupancy);
     GPE_BCASE(K_RK4_1)
     GPE_BCASE(K_RK4_2)
     GPE_BCASE(K_RK4_3)
@@ -285,9 +295,10 @@ static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStr
                ? batch_rk4_f32_rows()                                                                    \
                : 8;                                                                                      \
   }                                                                                                       \
-  cudaError_t launch_batch_##TAG(int kind, int grid, cudaStream_t st, const BatchStage* tab,            \
+  cudaError_t launch_batch_##TAG(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab,     \
                                  const BatchItem* items, const int* order, int nitems, int* queue,     \
                                  double* partials, int* occupancy) {                                   \
-    return launch_batch_impl<S, C>(kind, grid, st, tab, items, order, nitems, queue, partials, occupancy); \
+    return launch_batch_impl<S, C>(kind, R, grid, st, tab, items, order, nitems, queue, partials,       \
+                                   occupancy);                                                          \
   }                                                                                                     \
   }

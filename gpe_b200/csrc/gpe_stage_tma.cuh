@@ -746,15 +746,19 @@ __host__ __device__ constexpr int batch_threads() {
 
 // PAIR (complex64 storage with the FP32 stencil only): 16 x 8 threads, each
 // with two x-adjacent sites in TY/8 rows of the 32 x TY item tile
-// (tma_item_pair); otherwise 32 x TY/PY threads with PY rows each.
-template <class S, class C, int KIND, int TY, int PY, bool PAIR = false>
+// (tma_item_pair); otherwise 32 x TY/PY threads with PY rows each.  RR is
+// the stencil radius of every solve the launch serves (a pool keeps solves
+// of the two FD orders in separate classes): one item body per kernel, and
+// rings sized for that radius.
+template <class S, class C, int KIND, int TY, int PY, bool PAIR, int RR>
 __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_blocks<C, KIND, PAIR ? TY : 8>()))
     k_stage_batch(const BatchStage* __restrict__ tab, const BatchItem* __restrict__ items,
                   const int* __restrict__ order, int nitems, int* queue, double* partials) {
   static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && (TY == 8 || TY == 16)),
                 "the pair layout is for complex64 / FP32 on 32 x 8 or 32 x 16 items");
+  static_assert(RR == 1 || RR == 2, "stencil radius 1 or 2");
   constexpr int PYP = TY / 8;  // rows per thread of the pair layout
-  using LY = TmaLayout<S, 2, StageTraits<KIND>::NPW, TY>;
+  using LY = TmaLayout<S, RR, StageTraits<KIND>::NPW, TY>;
   constexpr int NT = batch_threads<TY, PY, PAIR>();
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
@@ -781,24 +785,14 @@ __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_bloc
     // every thread); a shared-memory copy would be re-read after every
     // barrier of the z march
     const StageArgs sa = __ldg_args(&bs->args);
-    const int R = sa.R;
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;
-    if constexpr (PAIR) {
-      if (R == 1)
-        ok = tma_item_pair<C, 1, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                    r_err);
-      else
-        ok = tma_item_pair<C, 2, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                    r_err);
-    } else {
-      if (R == 1)
-        ok = tma_item<S, C, 1, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                 r_err);
-      else
-        ok = tma_item<S, C, 2, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                 r_err);
-    }
+    if constexpr (PAIR)
+      ok = tma_item_pair<C, RR, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                   r_err);
+    else
+      ok = tma_item<S, C, RR, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                r_err);
     if (!ok) return;
     if (partials) block_reduce_store_at<NT>(r_norm, r_en, r_err, partials, w);
   }
