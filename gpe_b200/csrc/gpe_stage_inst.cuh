@@ -164,14 +164,16 @@ inline bool batch_pair_layout() {
 }
 
 // Item rows of the batched RK4 kernels for complex64 storage with the FP32
-// stencil: 32 x 8 items (one row of x pairs per thread); GPE_BATCH_ROWS=16
-// selects 32 x 16 items with two rows per thread (no faster on an uneven
-// mix of 32^3-160^3 solves: 40.1 against 40.5 G site-updates/s).  Every
-// other class uses 32 x 8 items.
+// stencil: 32 x 16 items with two rows of x pairs per thread (four sites),
+// as the single-solve kernel; GPE_BATCH_ROWS=8 selects 32 x 8 items with one
+// row per thread.  With one stencil radius per kernel the four-site body
+// fits 4 CTAs per SM without spills: 44.0-44.3 against 42.4-42.6 G
+// site-updates/s on the uneven mix of 32^3-160^3 solves.  Every other class
+// uses 32 x 8 items.
 inline int batch_rk4_f32_rows() {
   static const int rows = [] {
     const char* e = getenv("GPE_BATCH_ROWS");
-    return (e && atoi(e) == 16) && batch_pair_layout() ? 16 : 8;
+    return (e && atoi(e) == 8) || !batch_pair_layout() ? 8 : 16;
   }();
   return rows;
 }
