@@ -51,12 +51,9 @@ enum TileVariant : int {
   TILE_32x8_ROW2 = 4,    // 32 x 4 threads, two rows each
   TILE_PAIR_32x8 = 16,   // 16 x 8 threads, one x pair each
   TILE_PAIR_32x16 = 32,  // 16 x 8 threads on a 32 x 16 tile, an x pair in two rows each
-  TILE_PAIR_32x16_ZS = 48,  // the same with z neighbours read from the shared-memory ring
 };
-__host__ __device__ constexpr int tile_rows(int v) { return (v == TILE_PAIR_32x16 || v == TILE_PAIR_32x16_ZS) ? 16 : 8; }
-__host__ __device__ constexpr bool tile_is_pair(int v) {
-  return v == TILE_PAIR_32x8 || v == TILE_PAIR_32x16 || v == TILE_PAIR_32x16_ZS;
-}
+__host__ __device__ constexpr int tile_rows(int v) { return v == TILE_PAIR_32x16 ? 16 : 8; }
+__host__ __device__ constexpr bool tile_is_pair(int v) { return v == TILE_PAIR_32x8 || v == TILE_PAIR_32x16; }
 
 // reduction slots in the per-block partials: [norm, energy, errmax]
 enum { RED_NORM = 0, RED_ENERGY = 1, RED_ERR = 2, RED_SLOTS = 3 };

@@ -432,7 +432,7 @@ __device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool ac
     *p = v0;
 }
 
-template <class C, int R, int KIND, int TY, int PY, class LY, bool ZS = false>
+template <class C, int R, int KIND, int TY, int PY, class LY>
 __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                               TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                               double& r_err) {
@@ -522,11 +522,9 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
 #pragma unroll
   for (int l = 0; l < 2 * R; ++l) {
     ok &= swait(l);
-    if constexpr (!ZS) {
-      const S* tl = stile(l);
+    const S* tl = stile(l);
 #pragma unroll
-      for (int r = 0; r < PY; ++r) q[r][l] = lds_pair(tl + cofs[r]);
-    }
+    for (int r = 0; r < PY; ++r) q[r][l] = lds_pair(tl + cofs[r]);
   }
   if (!ok) *s_abort = 1;
   __syncthreads();
@@ -534,13 +532,10 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     drain(0, 0);
     return false;
   }
-  if constexpr (!ZS) {
-    // the slots of the planes only the queue needed are refilled at once
-    if (tid == 0) {
-      fence_proxy_async();
-      for (int l = 0; l < R; ++l)
-        if (l + NSS < L) issue_stencil(l + NSS);
-    }
+  if (tid == 0) {
+    fence_proxy_async();
+    for (int l = 0; l < R; ++l)
+      if (l + NSS < L) issue_stencil(l + NSS);
   }
 
   int sl_s = (SB + 2 * R) % NSS, sl_p = ((SB + 2 * R) / NSS) & 1;
@@ -551,7 +546,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
     bool okw = mbar_wait_bounded(&rg.sbar[sl_s], sl_p);
-    if constexpr (!ZS) {
+    {
       const S* tl = (const S*)(rg.sring + sl_s * LY::ST_SLOT);
 #pragma unroll
       for (int r = 0; r < PY; ++r) q[r][2 * R] = lds_pair(tl + cofs[r]);
@@ -575,20 +570,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
 #pragma unroll
       for (int r = 0; r < PY; ++r) {
         const S* c = tile + cofs[r];
-        // z neighbours: the register queue, or (ZS) the ring slots of the
-        // planes k-R .. k+R, which stay resident until the march leaves them
-        float4 zq[2 * R + 1];
-        if constexpr (ZS) {
-#pragma unroll
-          for (int d = 0; d <= 2 * R; ++d) {
-            const int sd = (sc_s + d - R + NSS) % NSS;
-            zq[d] = lds_pair((const S*)(rg.sring + sd * LY::ST_SLOT) + cofs[r]);
-          }
-        } else {
-#pragma unroll
-          for (int d = 0; d <= 2 * R; ++d) zq[d] = q[r][d];
-        }
-        const float4 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = zq[R];
+        const float4 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = q[r][R];
         const float4 ym1 = lds_pair(c - TW), yp1 = lds_pair(c + TW);
         Nb<C> n0, n1;
         n0.c0 = to_c<C>(lo2(cc4));
@@ -601,10 +583,10 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
         n1.ym1 = to_c<C>(hi2(ym1));
         n0.yp1 = to_c<C>(lo2(yp1));
         n1.yp1 = to_c<C>(hi2(yp1));
-        n0.zm1 = to_c<C>(lo2(zq[R - 1]));
-        n1.zm1 = to_c<C>(hi2(zq[R - 1]));
-        n0.zp1 = to_c<C>(lo2(zq[R + 1]));
-        n1.zp1 = to_c<C>(hi2(zq[R + 1]));
+        n0.zm1 = to_c<C>(lo2(q[r][R - 1]));
+        n1.zm1 = to_c<C>(hi2(q[r][R - 1]));
+        n0.zp1 = to_c<C>(lo2(q[r][R + 1]));
+        n1.zp1 = to_c<C>(hi2(q[r][R + 1]));
         if constexpr (R == 2) {
           const float4 ym2 = lds_pair(c - 2 * TW), yp2 = lds_pair(c + 2 * TW);
           n0.xm2 = to_c<C>(lo2(xl));
@@ -615,10 +597,10 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
           n1.ym2 = to_c<C>(hi2(ym2));
           n0.yp2 = to_c<C>(lo2(yp2));
           n1.yp2 = to_c<C>(hi2(yp2));
-          n0.zm2 = to_c<C>(lo2(zq[0]));
-          n1.zm2 = to_c<C>(hi2(zq[0]));
-          n0.zp2 = to_c<C>(lo2(zq[4]));
-          n1.zp2 = to_c<C>(hi2(zq[4]));
+          n0.zm2 = to_c<C>(lo2(q[r][0]));
+          n1.zm2 = to_c<C>(hi2(q[r][0]));
+          n0.zp2 = to_c<C>(lo2(q[r][4]));
+          n1.zp2 = to_c<C>(hi2(q[r][4]));
         } else {
           n0.xm2 = n0.xp2 = n0.ym2 = n0.yp2 = n0.zm2 = n0.zp2 = cx<C>{0, 0};
           n1.xm2 = n1.xp2 = n1.ym2 = n1.yp2 = n1.zm2 = n1.zp2 = cx<C>{0, 0};
@@ -676,10 +658,8 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     }
 #pragma unroll
     for (int r = 0; r < PY; ++r) {
-      if constexpr (!ZS) {
 #pragma unroll
-        for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
-      }
+      for (int d = 0; d < 2 * R; ++d) q[r][d] = q[r][d + 1];
       o[r] += g.pz;
     }
     if (++sl_s == NSS) { sl_s = 0; sl_p ^= 1; }
@@ -693,10 +673,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
     }
     if (tid == 0) {
       fence_proxy_async();
-      // the slot of the plane the march no longer reads: the centre (queue)
-      // or the lowest of the 2R+1 planes (ZS)
-      const int lfree = ZS ? m : lc;
-      if (lfree + NSS < L) issue_stencil(lfree + NSS);
+      if (lc + NSS < L) issue_stencil(lc + NSS);
       if (m + NPS < M) issue_pw(m + NPS);
     }
   }
@@ -707,7 +684,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
 
 // Single-solve stage kernel with two x-adjacent sites per thread
 // (complex64 storage): one work item per CTA, 16 x TY/PY threads.
-template <class C, int R, int KIND, int TY, int PY, bool ZS = false>
+template <class C, int R, int KIND, int TY, int PY>
 __global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_constant__ TmaMaps maps,
                                                                 const StageArgs a) {
   using LY = TmaLayout<float2, R, StageTraits<KIND>::NPW, TY>;
@@ -715,8 +692,8 @@ __global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_co
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item_pair<C, R, KIND, TY, PY, LY, ZS>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort,
-                                                 r_norm, r_en, r_err))
+  if (!tma_item_pair<C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+                                             r_en, r_err))
     return;
   if (a.partials) block_reduce_store<16 * TY / PY>(r_norm, r_en, r_err, a.partials);
 }

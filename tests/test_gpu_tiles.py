@@ -22,7 +22,7 @@ from oracle.pyoracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-LAYOUTS = {"row2": "4", "pair_32x8": "16", "pair_32x16": "32", "pair_32x16_zs": "48"}
+LAYOUTS = {"row2": "4", "pair_32x8": "16", "pair_32x16": "32"}
 
 
 def run_with(layout, rp, psi0, steps, **kw):
@@ -54,7 +54,7 @@ def test_pair_layouts_equal_row_layout_bitwise(gpu, shape, order, bcs, scheme):
     rng = np.random.default_rng(nx * 131 + ny * 7 + nz + order + bcs)
     psi0 = (1.0 + 0.2 * (rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx)))).astype(np.complex64)
     ref, iref, eref = run_with("row2", rp, psi0, 6, want_norm=True, want_energy=True)
-    for layout in ("pair_32x8", "pair_32x16", "pair_32x16_zs"):
+    for layout in ("pair_32x8", "pair_32x16"):
         out, info, e = run_with(layout, rp, psi0, 6, want_norm=True, want_energy=True)
         np.testing.assert_array_equal(out, ref)
         # the per-CTA partial sums follow the tile shape, so the reductions
