@@ -684,8 +684,7 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
   if (const char* e = getenv("GPE_ROWS_PER_THREAD")) h->tma_ty = atoi(e) == 1 ? TILE_32x8_ROW1 : TILE_32x8_ROW2;
   if (const char* e = getenv("GPE_TILE")) {
     const int v = atoi(e);
-    if (v == TILE_32x8_ROW1 || v == TILE_32x8_ROW2 || (h->cmode == CM_F32 && h->use_tma && tile_is_pair(v)) ||
-        (h->cmode == CM_F64 && h->use_tma && v == TILE_PAIR_32x8))
+    if (v == TILE_32x8_ROW1 || v == TILE_32x8_ROW2 || (h->cmode == CM_F32 && h->use_tma && tile_is_pair(v)))
       h->tma_ty = v;
   }
   const int th = tile_rows(h->tma_ty);

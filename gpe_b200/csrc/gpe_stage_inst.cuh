@@ -85,29 +85,29 @@ static cudaError_t launch_tma_kind(int kind, dim3 grid, cudaStream_t st, const T
   }
 }
 
-template <class S, class C, int R, int K, int TY, int PY>
+template <class C, int R, int K, int TY, int PY>
 static cudaError_t launch_tma_pair_one(dim3 grid, cudaStream_t st, const TmaMaps& m, const StageArgs& a) {
-  using LY = TmaLayout<S, R, StageTraits<K>::NPW, TY>;
+  using LY = TmaLayout<float2, R, StageTraits<K>::NPW, TY>;
   static unsigned long long attr_set = 0;  // per instantiation, one bit per device
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !(attr_set & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_tma_pair<S, C, R, K, TY, PY>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage_tma_pair<C, R, K, TY, PY>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_set |= 1ULL << dev;
   }
-  k_stage_tma_pair<S, C, R, K, TY, PY><<<grid, dim3(16, TY / PY), LY::SMEM, st>>>(m, a);
+  k_stage_tma_pair<C, R, K, TY, PY><<<grid, dim3(16, TY / PY), LY::SMEM, st>>>(m, a);
   return cudaGetLastError();
 }
 
-template <class S, class C, int R, int TY, int PY>
+template <class C, int R, int TY, int PY>
 static cudaError_t launch_tma_pair_kind(int kind, dim3 grid, cudaStream_t st, const TmaMaps& m,
                                         const StageArgs& a) {
   switch (kind) {
 #define GPE_PCASE(K) \
   case K:            \
-    return launch_tma_pair_one<S, C, R, K, TY, PY>(grid, st, m, a);
+    return launch_tma_pair_one<C, R, K, TY, PY>(grid, st, m, a);
     GPE_PCASE(K_EULER)
     GPE_PCASE(K_RK2_1)
     GPE_PCASE(K_RK2_2)
@@ -132,21 +132,14 @@ template <class S, class C>
 static cudaError_t launch_stage_tma_impl(int kind, int R, int ty, dim3 grid, cudaStream_t st, const TmaMaps& m,
                                          const StageArgs& a) {
   // ty is a TileVariant: TILE_32x8_ROW1 / TILE_32x8_ROW2 (any storage), or
-  // the pair layouts: complex64 storage with FP32 stencil compute (32 x 8
-  // and 32 x 16 tiles), complex128 with FP64 (32 x 8 tiles)
+  // the pair layouts (complex64 storage with FP32 stencil compute)
   if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
     if (ty == TILE_PAIR_32x8) {
-      if (R == 1) return launch_tma_pair_kind<S, C, 1, 8, 1>(kind, grid, st, m, a);
-      if (R == 2) return launch_tma_pair_kind<S, C, 2, 8, 1>(kind, grid, st, m, a);
+      if (R == 1) return launch_tma_pair_kind<C, 1, 8, 1>(kind, grid, st, m, a);
+      if (R == 2) return launch_tma_pair_kind<C, 2, 8, 1>(kind, grid, st, m, a);
     } else if (ty == TILE_PAIR_32x16) {
-      if (R == 1) return launch_tma_pair_kind<S, C, 1, 16, 2>(kind, grid, st, m, a);
-      if (R == 2) return launch_tma_pair_kind<S, C, 2, 16, 2>(kind, grid, st, m, a);
-    }
-  }
-  if constexpr (std::is_same<S, double2>::value && std::is_same<C, double>::value) {
-    if (ty == TILE_PAIR_32x8) {
-      if (R == 1) return launch_tma_pair_kind<S, C, 1, 8, 1>(kind, grid, st, m, a);
-      if (R == 2) return launch_tma_pair_kind<S, C, 2, 8, 1>(kind, grid, st, m, a);
+      if (R == 1) return launch_tma_pair_kind<C, 1, 16, 2>(kind, grid, st, m, a);
+      if (R == 2) return launch_tma_pair_kind<C, 2, 16, 2>(kind, grid, st, m, a);
     }
   }
   if (ty == 8) {

@@ -421,27 +421,9 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
 // outputs leave as 16-byte stores.  The per-site arithmetic is sites_stage,
 // the same as the one-site-per-column kernels, so results are identical.
 // ---------------------------------------------------------------------------
-// Two x-adjacent complex values: one 16-byte word for complex64, two
-// 16-byte words for complex128.
-template <class S>
-struct PairOf;
-template <>
-struct PairOf<float2> {
-  float4 v;
-  __device__ __forceinline__ float2 lo() const { return make_float2(v.x, v.y); }
-  __device__ __forceinline__ float2 hi() const { return make_float2(v.z, v.w); }
-};
-template <>
-struct PairOf<double2> {
-  double2 a, b;
-  __device__ __forceinline__ double2 lo() const { return a; }
-  __device__ __forceinline__ double2 hi() const { return b; }
-};
-
-__device__ __forceinline__ PairOf<float2> lds_pair(const float2* p) {
-  return PairOf<float2>{*reinterpret_cast<const float4*>(p)};
-}
-__device__ __forceinline__ PairOf<double2> lds_pair(const double2* p) { return PairOf<double2>{p[0], p[1]}; }
+__device__ __forceinline__ float4 lds_pair(const float2* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
 // store the sites (i, i+1) of a pair; i+1 inside the grid implies i is
 __device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool act0, bool act1) {
   if (act1)
@@ -449,23 +431,19 @@ __device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool ac
   else if (act0)
     *p = v0;
 }
-__device__ __forceinline__ void st_pair(double2* p, double2 v0, double2 v1, bool act0, bool act1) {
-  if (act0) p[0] = v0;
-  if (act1) p[1] = v1;
-}
 
-template <class S, class C, int R, int KIND, int TY, int PY, class LY>
+template <class C, int R, int KIND, int TY, int PY, class LY>
 __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                               TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                               double& r_err) {
+  using S = float2;
   using T = StageTraits<KIND>;
-  using P2 = PairOf<S>;
   constexpr int TX = TMA_TX, HX = TMA_HX, TW = tma_stencil_w(), TXT = TX / 2, TYT = TY / PY;
   constexpr int NSS = LY::NSS, NPS = LY::NPS, NPW = T::NPW;
   constexpr int NS = 2 * PY;  // sites per thread: site 2r + s is x = i0 + s of owned row r
   constexpr uint32_t ST_BYTES = tma_st_bytes<S>(R, TY), PW1 = tma_pw1_bytes<S>(TY);
   static_assert(TY % PY == 0, "PY must divide TY");
-  static_assert(HX % 2 == 0 && TW % 2 == 0, "pairs must stay aligned in the tiles");
+  static_assert(HX % 2 == 0 && TW % 2 == 0, "pairs must stay 16-byte aligned in the tiles");
 
   const Geom& g = a.g;
   const int tx = threadIdx.x, tyt = threadIdx.y, tid = tyt * TXT + tx;
@@ -538,7 +516,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
                    (by * TY + TY - 1 >= g.ny - 1 - R);
 
   auto stile = [&](int l) { return (const S*)(rg.sring + ((SB + l) % NSS) * LY::ST_SLOT); };
-  P2 q[PY][2 * R + 1];  // z queue of each owned row's pair: planes k-R .. k+R
+  float4 q[PY][2 * R + 1];  // z queue of each owned row's pair: planes k-R .. k+R
   bool ok = true;
   if (*(volatile const int*)a.status == STATUS_EXPIRE_TEST) ok = mbar_wait_bounded(rg.nbar, 0, EXPIRE_TEST_POLLS);
 #pragma unroll
@@ -592,37 +570,37 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
 #pragma unroll
       for (int r = 0; r < PY; ++r) {
         const S* c = tile + cofs[r];
-        const P2 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = q[r][R];
-        const P2 ym1 = lds_pair(c - TW), yp1 = lds_pair(c + TW);
+        const float4 xl = lds_pair(c - 2), xr = lds_pair(c + 2), cc4 = q[r][R];
+        const float4 ym1 = lds_pair(c - TW), yp1 = lds_pair(c + TW);
         Nb<C> n0, n1;
-        n0.c0 = to_c<C>((cc4).lo());
-        n1.c0 = to_c<C>((cc4).hi());
-        n0.xm1 = to_c<C>((xl).hi());
-        n0.xp1 = to_c<C>((cc4).hi());
-        n1.xm1 = to_c<C>((cc4).lo());
-        n1.xp1 = to_c<C>((xr).lo());
-        n0.ym1 = to_c<C>((ym1).lo());
-        n1.ym1 = to_c<C>((ym1).hi());
-        n0.yp1 = to_c<C>((yp1).lo());
-        n1.yp1 = to_c<C>((yp1).hi());
-        n0.zm1 = to_c<C>((q[r][R - 1]).lo());
-        n1.zm1 = to_c<C>((q[r][R - 1]).hi());
-        n0.zp1 = to_c<C>((q[r][R + 1]).lo());
-        n1.zp1 = to_c<C>((q[r][R + 1]).hi());
+        n0.c0 = to_c<C>(lo2(cc4));
+        n1.c0 = to_c<C>(hi2(cc4));
+        n0.xm1 = to_c<C>(hi2(xl));
+        n0.xp1 = to_c<C>(hi2(cc4));
+        n1.xm1 = to_c<C>(lo2(cc4));
+        n1.xp1 = to_c<C>(lo2(xr));
+        n0.ym1 = to_c<C>(lo2(ym1));
+        n1.ym1 = to_c<C>(hi2(ym1));
+        n0.yp1 = to_c<C>(lo2(yp1));
+        n1.yp1 = to_c<C>(hi2(yp1));
+        n0.zm1 = to_c<C>(lo2(q[r][R - 1]));
+        n1.zm1 = to_c<C>(hi2(q[r][R - 1]));
+        n0.zp1 = to_c<C>(lo2(q[r][R + 1]));
+        n1.zp1 = to_c<C>(hi2(q[r][R + 1]));
         if constexpr (R == 2) {
-          const P2 ym2 = lds_pair(c - 2 * TW), yp2 = lds_pair(c + 2 * TW);
-          n0.xm2 = to_c<C>((xl).lo());
-          n1.xm2 = to_c<C>((xl).hi());
-          n0.xp2 = to_c<C>((xr).lo());
-          n1.xp2 = to_c<C>((xr).hi());
-          n0.ym2 = to_c<C>((ym2).lo());
-          n1.ym2 = to_c<C>((ym2).hi());
-          n0.yp2 = to_c<C>((yp2).lo());
-          n1.yp2 = to_c<C>((yp2).hi());
-          n0.zm2 = to_c<C>((q[r][0]).lo());
-          n1.zm2 = to_c<C>((q[r][0]).hi());
-          n0.zp2 = to_c<C>((q[r][4]).lo());
-          n1.zp2 = to_c<C>((q[r][4]).hi());
+          const float4 ym2 = lds_pair(c - 2 * TW), yp2 = lds_pair(c + 2 * TW);
+          n0.xm2 = to_c<C>(lo2(xl));
+          n1.xm2 = to_c<C>(hi2(xl));
+          n0.xp2 = to_c<C>(lo2(xr));
+          n1.xp2 = to_c<C>(hi2(xr));
+          n0.ym2 = to_c<C>(lo2(ym2));
+          n1.ym2 = to_c<C>(hi2(ym2));
+          n0.yp2 = to_c<C>(lo2(yp2));
+          n1.yp2 = to_c<C>(hi2(yp2));
+          n0.zm2 = to_c<C>(lo2(q[r][0]));
+          n1.zm2 = to_c<C>(hi2(q[r][0]));
+          n0.zp2 = to_c<C>(lo2(q[r][4]));
+          n1.zp2 = to_c<C>(hi2(q[r][4]));
         } else {
           n0.xm2 = n0.xp2 = n0.ym2 = n0.yp2 = n0.zm2 = n0.zp2 = cx<C>{0, 0};
           n1.xm2 = n1.xp2 = n1.ym2 = n1.yp2 = n1.zm2 = n1.zp2 = cx<C>{0, 0};
@@ -638,9 +616,9 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
         }
 #pragma unroll
         for (int f = 0; f < NPW; ++f) {
-          const P2 w = lds_pair(pws + f * (TX * TY) + pofs[r]);
-          pv[2 * r][f] = (w).lo();
-          pv[2 * r + 1][f] = (w).hi();
+          const float4 w = lds_pair(pws + f * (TX * TY) + pofs[r]);
+          pv[2 * r][f] = lo2(w);
+          pv[2 * r + 1][f] = hi2(w);
         }
       }
       S ns[NS], ax[NS];
@@ -706,16 +684,16 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
 
 // Single-solve stage kernel with two x-adjacent sites per thread
 // (complex64 storage): one work item per CTA, 16 x TY/PY threads.
-template <class S, class C, int R, int KIND, int TY, int PY>
+template <class C, int R, int KIND, int TY, int PY>
 __global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_constant__ TmaMaps maps,
                                                                 const StageArgs a) {
-  using LY = TmaLayout<S, R, StageTraits<KIND>::NPW, TY>;
+  using LY = TmaLayout<float2, R, StageTraits<KIND>::NPW, TY>;
   extern __shared__ unsigned char smem_raw[];
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item_pair<S, C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort,
-                                                r_norm, r_en, r_err))
+  if (!tma_item_pair<C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+                                             r_en, r_err))
     return;
   if (a.partials) block_reduce_store<16 * TY / PY>(r_norm, r_en, r_err, a.partials);
 }
@@ -810,8 +788,8 @@ __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_bloc
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
     bool ok;
     if constexpr (PAIR)
-      ok = tma_item_pair<S, C, RR, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
-                                                      r_en, r_err);
+      ok = tma_item_pair<C, RR, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                   r_err);
     else
       ok = tma_item<S, C, RR, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
                                                 r_err);

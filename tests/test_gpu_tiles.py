@@ -76,36 +76,3 @@ def test_pair_layout_other_equations_with_urhs_and_diss(gpu, eqn):
     # and the layout is within the FP32 bar of the FP64 oracle
     o = Oracle(rp.replace(storage="c128", compute="auto")).run(psi0.astype(np.complex128), 5)
     assert float(np.linalg.norm((out - o).ravel()) / np.linalg.norm(o.ravel())) <= 1e-5
-
-
-@pytest.mark.parametrize("order,bcs", [(2, 1), (2, 2), (4, 1), (4, 2)])
-@pytest.mark.parametrize("scheme", ["rk4", "rk45"])
-def test_fp64_pair_layout_equals_row_layout_bitwise(gpu, order, bcs, scheme):
-    """complex128 with the two-sites-per-thread layout on 32 x 8 tiles
-    (GPE_TILE=16) against the default one-site-per-column layout."""
-    nx, ny, nz = 37, 21, 19
-    rp = RunParams(nx=nx, ny=ny, nz=nz, xr=0.5 * (nx - 1), yr=0.5 * (ny - 1), zr=0.5 * (nz - 1), tau=0.004,
-                   scheme=scheme, eqn_to_solve=4, bcs=bcs, order=order, g=1.0, mu=2.0, omx=0.3, omy=0.2, omz=0.25)
-    rng = np.random.default_rng(nx + order + bcs)
-    psi0 = 1.0 + 0.2 * (rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx)))
-
-    def run(layout):
-        old = os.environ.get("GPE_TILE")
-        os.environ["GPE_TILE"] = LAYOUTS[layout]
-        try:
-            s = Solver(rp)
-        finally:
-            if old is None:
-                del os.environ["GPE_TILE"]
-            else:
-                os.environ["GPE_TILE"] = old
-        s.set_state(psi0)
-        info = s.solver(6, want_norm=True)
-        out = s.get_state()
-        s.close()
-        return out, info
-
-    ref, iref = run("row2")
-    out, info = run("pair_32x8")
-    np.testing.assert_array_equal(out, ref)
-    assert info.norm == pytest.approx(iref.norm, rel=1e-13)
