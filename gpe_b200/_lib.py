@@ -57,7 +57,8 @@ class GpeStepInfo(C.Structure):
     ]
 
 
-GPE_IC_UNIFORM, GPE_IC_FERMI, GPE_IC_LINE, GPE_IC_RING, GPE_IC_LINE_PADE, GPE_IC_RANDOM_PHASE = range(6)
+(GPE_IC_UNIFORM, GPE_IC_FERMI, GPE_IC_LINE, GPE_IC_RING, GPE_IC_LINE_PADE, GPE_IC_RANDOM_PHASE, GPE_IC_PADE_PULSE,
+ GPE_IC_PADE_RING, GPE_IC_VORTEX_PAIR, GPE_IC_SPHERE, GPE_IC_SPHERE2, GPE_IC_WALL) = range(12)
 
 
 class GpeRing(C.Structure):
@@ -72,9 +73,14 @@ class GpeLine(C.Structure):
                 ("dir", C.c_char), ("reserved", C.c_char * 3)]
 
 
+class GpePulse(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double), ("r0", C.c_double)]
+
+
 class GpeIC(C.Structure):
     _fields_ = [("nfactors", C.c_int32), ("factor", C.c_int32 * 4), ("reserved", C.c_int32),
-                ("ring", GpeRing), ("line", GpeLine), ("seed", C.c_uint64), ("kc", C.c_double)]
+                ("ring", GpeRing), ("line", GpeLine), ("seed", C.c_uint64), ("kc", C.c_double),
+                ("pulse", GpePulse)]
 
 
 class GpeResult(C.Structure):

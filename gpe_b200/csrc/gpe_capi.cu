@@ -159,7 +159,7 @@ int fail(gpe_handle* h, int code, const std::string& msg) {
 int validate(const gpe_params* p, std::string& why) { return validate_params(p, why); }
 void layout(const gpe_params* p, Geom& g, int& esz) { param_layout(p, g, esz); }
 int nfields(int scheme) { return scheme_fields(scheme); }
-int choose_zc(const Geom& g, int tile_h) { return default_zc(g, tile_h); }
+int choose_zc(const Geom& g, int tile_h, int esz) { return default_zc(g, tile_h, esz); }
 bool encode_field_maps(gpe_handle* h, void* base, CUtensorMap* halo, CUtensorMap* pw) {
   return encode_maps(base, h->g, h->esz, h->R, halo, pw, tile_rows(h->tma_ty));
 }
@@ -688,7 +688,7 @@ int create_impl(const gpe_params* p, const SlabSpec* sp, gpe_handle** out) {
       h->tma_ty = v;
   }
   const int th = tile_rows(h->tma_ty);
-  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g, th);
+  h->zc = p->tile_zc > 0 ? std::min(p->tile_zc, pl.nz) : choose_zc(h->g, th, h->esz);
   h->grid = dim3((pl.nx + 31) / 32, (pl.ny + th - 1) / th, (pl.nz + h->zc - 1) / h->zc);
   h->npart = (long long)h->grid.x * h->grid.y * h->grid.z;
   h->norm_grid = dim3((pl.nx + 31) / 32, (pl.ny + 7) / 8, (pl.nz + h->zc - 1) / h->zc);

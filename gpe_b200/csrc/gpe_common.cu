@@ -57,18 +57,22 @@ int scheme_fields(int scheme) {
 }
 
 // z planes per block: enough blocks for several waves on 148 SMs
-int default_zc(const Geom& g, int tile_h) {
+int default_zc(const Geom& g, int tile_h, int esz) {
   if (const char* e = getenv("GPE_ZC")) {
     int v = atoi(e);
     if (v > 0) return std::min(v, g.nz);
   }
-  // at most 20 planes per CTA: at 256^3 the sweep 8..32 gives 20 the best
-  // rate (FP32 +1.4-1.8 %, FP64 +0.8 % over 16); small grids use fewer so
-  // that every SM gets several CTAs.
+  // at most 24 planes per CTA for complex128 sites (32x8 tiles) and 20 for
+  // complex64 (32x16 two-sites-per-thread tiles): at 256^3, sweeps of
+  // 16..43 planes give these the best rates (complex128: 24 is +0.7 % over
+  // 20 and 29, +3 % over 32; complex64: 20 is +1 % over 29, +2.4 % over 16,
+  // +3.4 % over 24); small grids use fewer so that every SM gets several
+  // CTAs.
   const long long bxy = (long long)((g.nx + 31) / 32) * ((g.ny + tile_h - 1) / tile_h);
   const long long target = 148LL * 8;
+  const long long cap = esz >= 16 ? 24 : 20;
   long long zc = (g.nz * bxy + target - 1) / target;
-  zc = std::max<long long>(4, std::min<long long>(zc, 20));
+  zc = std::max<long long>(4, std::min<long long>(zc, cap));
   return (int)std::min<long long>(zc, g.nz);
 }
 

@@ -23,7 +23,7 @@ long long padded_elems(const Geom& g);
 // fields a scheme keeps per solve
 int scheme_fields(int scheme);
 // z planes per CTA / work item
-int default_zc(const Geom& g, int tile_h = 8);
+int default_zc(const Geom& g, int tile_h = 8, int esz = 16);
 // tensor maps of one field: halo'd stencil box and point-wise box of a
 // 32 x tile_h tile
 bool encode_maps(void* base, const Geom& g, int esz, int R, CUtensorMap* halo, CUtensorMap* pw, int tile_h = 8);

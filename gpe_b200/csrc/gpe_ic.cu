@@ -77,6 +77,43 @@ __device__ __forceinline__ void ring_val(const gpe_ring& vr, double sc, double x
   *im = tr * z2i + ti * z2r;
 }
 
+// pade_pulse_ring (src/ic.f90:518-587): the Pade approximations of the
+// rarefaction pulse (pulse = true) and of the axisymmetric vortex ring that
+// move along x (N. G. Berloff, J. Phys. A 37, 1617 (2004)), centred at x0
+// with the axis through (y0, z0) and radius r0.  a(1..9), U and m are the
+// published coefficients the reference's get_consts lists for the two cases
+// (src/ic.f90:572-581); the same numbers give the same state.
+__device__ __forceinline__ void pade_val(bool pulse, const gpe_pulse& pp, double x, double y, double z, double* re,
+                                         double* im) {
+  const double a1 = pulse ? -0.79792 : -1.1, a2 = pulse ? 0.00388059 : 0.0170524;
+  const double a3 = pulse ? 0.00882276 : 0.0289452, a4 = pulse ? -0.7981 : -0.953;
+  const double a5 = pulse ? -0.012783 : -0.0049767, a6 = pulse ? -0.0574092 : -0.0594346;
+  const double a7 = pulse ? 0.0399 : 0.04, a8 = pulse ? 0.199 : 0.21, a9 = pulse ? 0.0058 : 0.00612;
+  const double U = pulse ? 0.63 : 0.6, m = pulse ? 8.37 : 8.97;
+  const double p74 = 7.0 / 4.0;
+  const double one_2u = 1.0 - 2.0 * (U * U);
+  const double ma9 = m * pow(a9, p74);
+  const double s = sqrt((y - pp.y0) * (y - pp.y0) + (z - pp.z0) * (z - pp.z0));  // get_s, ic.f90:804-820
+  const double xs = x - pp.x0;
+  const double x2 = xs * xs, s2 = (s - pp.r0) * (s - pp.r0);
+  const double t = x2 + one_2u * s2;
+  const double denom = pow(((1.0 + a8 * x2) + a7 * s2) + a9 * (t * t), p74);
+  *re = 1.0 + ((((a1 + a3 * x2) + a2 * s2) + (ma9 * U) * (2.0 * x2 - one_2u * s2)) * t) / denom;
+  *im = (xs * (((a4 + a6 * x2) + a5 * s2) - ma9 * (t * t))) / denom;
+}
+
+// vortex_pair (src/ic.f90:591-636): the Pade approximation of a vortex pair
+// in the x-y plane, the same in every z plane; coefficients as listed there.
+__device__ __forceinline__ void pair_val(double x, double y, double* re, double* im) {
+  const double a0 = -1.14026, a1 = -0.150112, a2 = -0.0294564;
+  const double b0 = -0.830953, b1 = -0.108296, b2 = -0.073641;
+  const double c0 = 0.35022, c1 = 0.03032, c2 = 0.15905, c3 = 0.04123, c4 = 0.01402;
+  const double x2 = x * x, y2 = y * y, x4 = x2 * x2, y4 = y2 * y2;
+  const double denom = ((((1.0 + c0 * x2) + c1 * x4) + c2 * y2) + (c3 * x2) * y2) + c4 * y4;
+  *re = 1.0 + ((a0 + a1 * x2) + a2 * y2) / denom;
+  *im = (x * ((b0 + b1 * x2) + b2 * y2)) / denom;
+}
+
 // The product of the closed-form factors of ic at (x, y, z), factors taken
 // left to right as the reference's init_cond expression multiplies them.
 __device__ __forceinline__ void ic_product(const gpe_ic& ic, const IcGrid& G, double x, double y, double z,
@@ -109,6 +146,22 @@ __device__ __forceinline__ void ic_product(const gpe_ic& ic, const IcGrid& G, do
         }
         case GPE_IC_RING:
           ring_val(ic.ring, G.scal, x, y, z, &fr, &fi);
+          break;
+        case GPE_IC_PADE_PULSE:
+        case GPE_IC_PADE_RING:
+          pade_val(ic.factor[q] == GPE_IC_PADE_PULSE, ic.pulse, x, y, z, &fr, &fi);
+          break;
+        case GPE_IC_VORTEX_PAIR:
+          pair_val(x, y, &fr, &fi);
+          break;
+        case GPE_IC_SPHERE:  // ic.f90:640-662 (rad = 10, eps1 = 2)
+          fr = 0.5 * (1.0 + tanh((sqrt((x * x + y * y) + z * z) - 10.0) - 2.0));
+          break;
+        case GPE_IC_SPHERE2:  // ic.f90:666-684 (amp = 100, width = 10)
+          fr = 100.0 * exp(-((x * x + y * y) + z * z) / 10.0);
+          break;
+        case GPE_IC_WALL:  // ic.f90:688-709 (pos = -30)
+          fr = z <= -30.0 ? 0.0 : 1.0;
           break;
         default:
           break;
@@ -277,7 +330,7 @@ int ic_validate(const gpe_ic* ic, std::string& why) {
   }
   for (int q = 0; q < ic->nfactors; ++q) {
     const int f = ic->factor[q];
-    if (f < GPE_IC_UNIFORM || f > GPE_IC_RANDOM_PHASE) {
+    if (f < GPE_IC_UNIFORM || f > GPE_IC_WALL) {
       why = "gpe_ic: unknown factor";
       return GPE_ERR_BADARG;
     }

@@ -334,17 +334,56 @@ gpe_ic parse_ic_in(const ParamsIn& P) {
   if (expr.empty()) emergency_stop("ERROR: ic.in has no active init_cond line");
   gpe_ic ic;
   memset(&ic, 0, sizeof(ic));
-  std::string f;
-  std::istringstream ss(expr);
-  while (std::getline(ss, f, '*')) {
-    f = trim(f);
+  bool have_pulse = false;
+  // factors are separated by '*' outside parentheses (an argument list
+  // may hold numbers like 1.0e-1_pr but no products)
+  std::vector<std::string> facs;
+  {
+    std::string cur;
+    int depth = 0;
+    for (char ch : expr) {
+      if (ch == '(') ++depth;
+      if (ch == ')') --depth;
+      if (ch == '*' && depth == 0) {
+        facs.push_back(trim(cur));
+        cur.clear();
+      } else {
+        cur += ch;
+      }
+    }
+    facs.push_back(trim(cur));
+  }
+  for (const std::string& f : facs) {
     if (ic.nfactors >= 4) emergency_stop("ERROR: ic.in product has more than four factors");
     int code;
     if (f.rfind("fermi", 0) == 0) code = GPE_IC_FERMI;
     else if (f.rfind("vortex_line", 0) == 0) code = GPE_IC_LINE;
     else if (f.rfind("vortex_ring", 0) == 0) code = GPE_IC_RING;
     else if (f.rfind("random_phase", 0) == 0) code = GPE_IC_RANDOM_PHASE;
-    else emergency_stop("ERROR: ic.in factor '" + f + "' is not supported");
+    else if (f.rfind("vortex_pair", 0) == 0) code = GPE_IC_VORTEX_PAIR;
+    else if (f.rfind("sphere2", 0) == 0) code = GPE_IC_SPHERE2;
+    else if (f.rfind("sphere", 0) == 0) code = GPE_IC_SPHERE;
+    else if (f.rfind("wall", 0) == 0) code = GPE_IC_WALL;
+    else if (f.rfind("pade_pulse_ring", 0) == 0) {
+      // pade_pulse_ring('pulse' | 'ring', x0, y0, z0, r0), src/ic.f90:518
+      const size_t a = f.find('('), b = f.rfind(')');
+      if (a == std::string::npos || b == std::string::npos || b < a)
+        emergency_stop("ERROR: ic.in factor '" + f + "' has no argument list");
+      const std::vector<std::string> args = fortran_args(f.substr(a + 1, b - a - 1));
+      if (args.size() != 5) emergency_stop("ERROR: pade_pulse_ring takes (pulse_or_ring, x0, y0, z0, r0)");
+      const std::string kind = lower(fstring(args[0]));
+      if (kind == "pulse") code = GPE_IC_PADE_PULSE;
+      else if (kind == "ring") code = GPE_IC_PADE_RING;
+      else emergency_stop("ERROR: pade_pulse_ring: pulse_or_ring must be 'pulse' or 'ring'");
+      const gpe_pulse pu{fnum(args[1], "pade_pulse_ring x0"), fnum(args[2], "pade_pulse_ring y0"),
+                         fnum(args[3], "pade_pulse_ring z0"), fnum(args[4], "pade_pulse_ring r0")};
+      if (have_pulse && (pu.x0 != ic.pulse.x0 || pu.y0 != ic.pulse.y0 || pu.z0 != ic.pulse.z0 || pu.r0 != ic.pulse.r0))
+        emergency_stop("ERROR: ic.in: two pade_pulse_ring factors with different arguments are not supported");
+      ic.pulse = pu;
+      have_pulse = true;
+    } else {
+      emergency_stop("ERROR: ic.in factor '" + f + "' is not supported");
+    }
     if (code == GPE_IC_LINE && !P.have_vl1) emergency_stop("ERROR: parameters.in has no vl1");
     if (code == GPE_IC_RING && !P.have_vr1) emergency_stop("ERROR: parameters.in has no vr1");
     ic.factor[ic.nfactors++] = code;
@@ -739,10 +778,12 @@ int main(int argc, char** argv) {
     printf("{\"nx\": %d, \"ny\": %d, \"nz\": %d, \"pr\": %d, \"scheme\": %d, \"eqn\": %d, \"bcs\": %d, "
            "\"order\": %d, \"real_time\": %d, \"tau\": %.17g, \"end_time\": %.17g, \"xr\": %.17g, \"g\": %.17g, "
            "\"mu\": %.17g, \"omz\": %.17g, \"save_rate\": %d, \"ic\": [%d, %d, %d, %d], \"nic\": %d, "
-           "\"ring_r0\": %.17g, \"ring_plane\": \"%c%c\", \"line_x0\": %.17g, \"line_dir\": \"%c\"}\n",
+           "\"ring_r0\": %.17g, \"ring_plane\": \"%c%c\", \"line_x0\": %.17g, \"line_dir\": \"%c\", "
+           "\"pulse\": [%.17g, %.17g, %.17g, %.17g]}\n",
            p.nx, p.ny, p.nz, c.P.pr, p.scheme, p.eqn, p.bcs, p.order, p.real_time, p.tau, c.r.end_time, p.xr, p.g,
            p.mu, p.omz, c.r.save_rate, ic.factor[0], ic.factor[1], ic.factor[2], ic.factor[3], ic.nfactors,
-           ic.ring.r0, ic.ring.plane[0], ic.ring.plane[1], ic.line.x0, ic.line.dir);
+           ic.ring.r0, ic.ring.plane[0], ic.ring.plane[1], ic.line.x0, ic.line.dir, ic.pulse.x0, ic.pulse.y0,
+           ic.pulse.z0, ic.pulse.r0);
     return 0;
   }
   if (c.r.imprint_vl && !c.P.have_vl1) emergency_stop("ERROR: imprint_vl=.true. but parameters.in has no vl1");

@@ -119,6 +119,70 @@ def fermi(p):
     return out.astype(np.complex128)
 
 
+# get_consts (src/ic.f90:563-585): the published Pade coefficients a(1..9),
+# velocity U and momentum m of the vortex ring and the rarefaction pulse
+_PADE = {
+    "ring": ((-1.1, 0.0170524, 0.0289452, -0.953, -0.0049767, -0.0594346, 0.04, 0.21, 0.00612), 0.6, 8.97),
+    "pulse": ((-0.79792, 0.00388059, 0.00882276, -0.7981, -0.012783, -0.0574092, 0.0399, 0.199, 0.0058), 0.63,
+              8.37),
+}
+
+
+def pade_pulse_ring(p, pulse_or_ring="pulse", x0=0.0, y0=0.0, z0=0.0, r0=0.0):
+    """pade_pulse_ring (src/ic.f90:518-587): the Pade approximation of a
+    rarefaction pulse ('pulse') or an axisymmetric vortex ring ('ring')
+    moving along x, centred at x0 with its axis through (y0, z0), radius r0
+    (N. G. Berloff, J. Phys. A 37, 1617 (2004))."""
+    a, U, m = _PADE[pulse_or_ring]
+    X, Y, Z = _mesh(p)
+    pw = 7.0 / 4.0
+    one_2u = 1.0 - 2.0 * (U * U)
+    ma9 = m * a[8] ** pw
+    s = np.sqrt((Y - y0) * (Y - y0) + (Z - z0) * (Z - z0))  # get_s (src/ic.f90:804-820)
+    xs = X - x0
+    x2 = xs * xs
+    s2 = (s - r0) * (s - r0)
+    t = x2 + one_2u * s2
+    denom = (((1.0 + a[7] * x2) + a[6] * s2) + a[8] * (t * t)) ** pw
+    uu = 1.0 + ((((a[0] + a[2] * x2) + a[1] * s2) + (ma9 * U) * (2.0 * x2 - one_2u * s2)) * t) / denom
+    vv = (xs * (((a[3] + a[5] * x2) + a[4] * s2) - ma9 * (t * t))) / denom
+    return np.ascontiguousarray(np.broadcast_to(uu + 1j * vv, (p.nz, p.ny, p.nx)), dtype=np.complex128)
+
+
+def vortex_pair(p):
+    """vortex_pair (src/ic.f90:591-636): Pade approximation of a vortex pair
+    in the x-y plane, the same in every z plane."""
+    a0, a1, a2 = -1.14026, -0.150112, -0.0294564
+    b0, b1, b2 = -0.830953, -0.108296, -0.073641
+    c0, c1, c2, c3, c4 = 0.35022, 0.03032, 0.15905, 0.04123, 0.01402
+    X, Y, _ = _mesh(p)
+    x2, y2 = X * X, Y * Y
+    denom = ((((1.0 + c0 * x2) + c1 * (x2 * x2)) + c2 * y2) + (c3 * x2) * y2) + c4 * (y2 * y2)
+    v = (1.0 + ((a0 + a1 * x2) + a2 * y2) / denom) + 1j * ((X * ((b0 + b1 * x2) + b2 * y2)) / denom)
+    return np.ascontiguousarray(np.broadcast_to(v, (p.nz, p.ny, p.nx)), dtype=np.complex128)
+
+
+def sphere(p):
+    """sphere (src/ic.f90:640-662): 0.5 (1 + tanh(r - rad - eps1)), rad = 10, eps1 = 2."""
+    X, Y, Z = _mesh(p)
+    v = 0.5 * (1.0 + np.tanh((np.sqrt((X * X + Y * Y) + Z * Z) - 10.0) - 2.0))
+    return np.ascontiguousarray(np.broadcast_to(v, (p.nz, p.ny, p.nx)), dtype=np.complex128)
+
+
+def sphere2(p):
+    """sphere2 (src/ic.f90:666-684): amp exp(-r^2/width), amp = 100, width = 10."""
+    X, Y, Z = _mesh(p)
+    v = 100.0 * np.exp(-((X * X + Y * Y) + Z * Z) / 10.0)
+    return np.ascontiguousarray(np.broadcast_to(v, (p.nz, p.ny, p.nx)), dtype=np.complex128)
+
+
+def wall(p):
+    """wall (src/ic.f90:688-709): 0 for z <= pos, else 1, pos = -30."""
+    _, _, Z = _mesh(p)
+    v = np.where(Z <= -30.0, 0.0, 1.0)
+    return np.ascontiguousarray(np.broadcast_to(v, (p.nz, p.ny, p.nx)), dtype=np.complex128)
+
+
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _M1 = np.uint64(0xBF58476D1CE4E5B9)
 _M2 = np.uint64(0x94D049BB133111EB)
@@ -161,14 +225,20 @@ def random_phase(p, seed: int = 1234, kc: float = 1.5):
 # Device-side initial conditions: specs for gpe_set_ic / gpe_pool_submit_ic
 
 
-def device_spec(*factors, ring=None, line=None, seed: int = 1234, kc: float = 1.5):
+def device_spec(*factors, ring=None, line=None, pulse=None, seed: int = 1234, kc: float = 1.5):
     """Build a gpe_ic spec: the product of the named factors ("uniform",
-    "fermi", "line", "ring", "line_pade", "random_phase").  ring / line are
-    dicts with the fields of ring_param / line_param (src/parameters.in)."""
+    "fermi", "line", "ring", "line_pade", "random_phase", "pade_pulse",
+    "pade_ring", "vortex_pair", "sphere", "sphere2", "wall").  ring / line
+    are dicts with the fields of ring_param / line_param
+    (src/parameters.in); pulse = dict(x0, y0, z0, r0), the arguments of
+    pade_pulse_ring."""
     from . import _lib as L
 
     codes = {"uniform": L.GPE_IC_UNIFORM, "fermi": L.GPE_IC_FERMI, "line": L.GPE_IC_LINE,
-             "ring": L.GPE_IC_RING, "line_pade": L.GPE_IC_LINE_PADE, "random_phase": L.GPE_IC_RANDOM_PHASE}
+             "ring": L.GPE_IC_RING, "line_pade": L.GPE_IC_LINE_PADE, "random_phase": L.GPE_IC_RANDOM_PHASE,
+             "pade_pulse": L.GPE_IC_PADE_PULSE, "pade_ring": L.GPE_IC_PADE_RING,
+             "vortex_pair": L.GPE_IC_VORTEX_PAIR, "sphere": L.GPE_IC_SPHERE, "sphere2": L.GPE_IC_SPHERE2,
+             "wall": L.GPE_IC_WALL}
     spec = L.GpeIC()
     spec.nfactors = len(factors)
     for q, f in enumerate(factors):
@@ -181,6 +251,10 @@ def device_spec(*factors, ring=None, line=None, seed: int = 1234, kc: float = 1.
     ln.update(line or {})
     for k, v in ln.items():
         setattr(spec.line, k, v.encode() if k == "dir" else (int(v) if k == "imprint_phase" else v))
+    pu = dict(x0=0.0, y0=0.0, z0=0.0, r0=0.0)
+    pu.update(pulse or {})
+    for k, v in pu.items():
+        setattr(spec.pulse, k, float(v))
     spec.seed = int(seed)
     spec.kc = float(kc)
     return spec

@@ -174,6 +174,14 @@ int gpe_get_stream(const gpe_handle* h, void** stream);
 #define GPE_IC_LINE_PADE 4    /* straight line with the Pade core r*get_rr(r)     */
 #define GPE_IC_RANDOM_PHASE 5 /* seeded spectrum |k| < kc, inverse FFT, mean
                                  density 1 (must be the only factor)               */
+#define GPE_IC_PADE_PULSE 6   /* pade_pulse_ring('pulse', x0, y0, z0, r0): Pade
+                                 rarefaction pulse moving along x, ic.f90:518      */
+#define GPE_IC_PADE_RING 7    /* pade_pulse_ring('ring', x0, y0, z0, r0): Pade
+                                 axisymmetric vortex ring moving along x, :518     */
+#define GPE_IC_VORTEX_PAIR 8  /* vortex_pair(): Pade vortex pair in x-y, :591     */
+#define GPE_IC_SPHERE 9       /* sphere(): 0.5(1 + tanh(r - 12)), :640            */
+#define GPE_IC_SPHERE2 10     /* sphere2(): 100 exp(-r^2/10), :666                */
+#define GPE_IC_WALL 11        /* wall(): 0 for z <= -30, else 1, :688             */
 
 typedef struct {              /* ring_param, src/parameters.in:54-68 */
   double x0, y0, z0, r0, amp, r1, dir;
@@ -189,6 +197,11 @@ typedef struct {              /* line_param, src/parameters.in:32-43 */
   char reserved[3];
 } gpe_line;
 
+typedef struct {              /* arguments of pade_pulse_ring, src/ic.f90:518-524 */
+  double x0, y0, z0;          /* centre; the axis of symmetry is the x line through (y0, z0) */
+  double r0;                  /* ring radius (distance of the core from the axis) */
+} gpe_pulse;
+
 typedef struct {
   int32_t nfactors;           /* 1..4 */
   int32_t factor[4];          /* GPE_IC_* */
@@ -197,6 +210,7 @@ typedef struct {
   gpe_line line;
   uint64_t seed;              /* GPE_IC_RANDOM_PHASE */
   double kc;                  /* GPE_IC_RANDOM_PHASE cutoff |k| < kc */
+  gpe_pulse pulse;            /* GPE_IC_PADE_PULSE / GPE_IC_PADE_RING (one set per product) */
 } gpe_ic;
 
 /* Set the handle's state to the initial condition (no host array). */

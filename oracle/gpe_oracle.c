@@ -938,6 +938,90 @@ void or_fermi(or_ctx *c, double *out) {
   free(v);
 }
 
+/* ic.f90:518-587 pade_pulse_ring.  get_consts (ic.f90:563-585) lists a(1..9),
+ * U and m for 'ring' and 'pulse'; denom, uu and vv are evaluated per site as
+ * the loop at ic.f90:537-555 writes them, with s = get_s (ic.f90:804-820). */
+int or_pade_pulse_ring(or_ctx *c, int pulse, double x0, double y0, double z0, double r0, double *out) {
+  static const double ring_a[9] = {-1.1, 0.0170524, 0.0289452, -0.953, -0.0049767, -0.0594346, 0.04, 0.21,
+                                   0.00612};
+  static const double pulse_a[9] = {-0.79792, 0.00388059, 0.00882276, -0.7981, -0.012783, -0.0574092, 0.0399,
+                                    0.199, 0.0058};
+  const double *a = pulse ? pulse_a : ring_a;
+  const double U = pulse ? 0.63 : 0.6, m = pulse ? 8.37 : 8.97;
+  const double pw = 7.0 / 4.0;
+  const double one_2u = 1.0 - 2.0 * (U * U);
+  const double a9p = pow(a[8], pw);
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++) {
+      double dy = c->y[j] - y0, dz = c->z[k] - z0;
+      double sjk = sqrt(dy * dy + dz * dz);
+      double s2 = (sjk - r0) * (sjk - r0);
+      for (int i = 0; i < c->nx; i++) {
+        double xs = c->x[i] - x0;
+        double x2 = xs * xs;
+        double t = x2 + one_2u * s2;
+        double denom = pow(((1.0 + a[7] * x2) + a[6] * s2) + a[8] * (t * t), pw);
+        double uu = 1.0 + ((((a[0] + a[2] * x2) + a[1] * s2) + ((m * a9p) * U) * (2.0 * x2 - one_2u * s2)) * t) /
+                              denom;
+        double vv = (xs * (((a[3] + a[5] * x2) + a[4] * s2) - (m * a9p) * (t * t))) / denom;
+        size_t n = IX(c, i, j, k);
+        out[2 * n] = uu;
+        out[2 * n + 1] = vv;
+      }
+    }
+  return 0;
+}
+
+/* ic.f90:591-636 vortex_pair (the same in every z plane) */
+void or_vortex_pair(or_ctx *c, double *out) {
+  const double a0 = -1.14026, a1 = -0.150112, a2 = -0.0294564;
+  const double b0 = -0.830953, b1 = -0.108296, b2 = -0.073641;
+  const double c0 = 0.35022, c1 = 0.03032, c2 = 0.15905, c3 = 0.04123, c4 = 0.01402;
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        double x = c->x[i], y = c->y[j];
+        double x2 = x * x, y2 = y * y;
+        double denom = ((((1.0 + c0 * x2) + c1 * (x2 * x2)) + c2 * y2) + (c3 * x2) * y2) + c4 * (y2 * y2);
+        size_t n = IX(c, i, j, k);
+        out[2 * n] = 1.0 + ((a0 + a1 * x2) + a2 * y2) / denom;
+        out[2 * n + 1] = (x * ((b0 + b1 * x2) + b2 * y2)) / denom;
+      }
+}
+
+/* ic.f90:640-662 sphere, 666-684 sphere2, 688-709 wall (real factors) */
+void or_sphere(or_ctx *c, double *out) {
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        double x = c->x[i], y = c->y[j], z = c->z[k];
+        size_t n = IX(c, i, j, k);
+        out[2 * n] = 0.5 * (1.0 + tanh((sqrt((x * x + y * y) + z * z) - 10.0) - 2.0));
+        out[2 * n + 1] = 0.0;
+      }
+}
+
+void or_sphere2(or_ctx *c, double *out) {
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        double x = c->x[i], y = c->y[j], z = c->z[k];
+        size_t n = IX(c, i, j, k);
+        out[2 * n] = 100.0 * exp(-((x * x + y * y) + z * z) / 10.0);
+        out[2 * n + 1] = 0.0;
+      }
+}
+
+void or_wall(or_ctx *c, double *out) {
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        size_t n = IX(c, i, j, k);
+        out[2 * n] = c->z[k] <= -30.0 ? 0.0 : 1.0;
+        out[2 * n + 1] = 0.0;
+      }
+}
+
 void or_cmul(const double *a, const double *b, double *out, int64_t n) {
   for (int64_t q = 0; q < n; q++) {
     double r, i;

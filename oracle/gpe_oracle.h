@@ -99,6 +99,13 @@ void or_fermi(or_ctx *c, double *out);
 void or_vtrap(or_ctx *c, double *out);
 /* straight vortex line with the Pade core R(r) = r*get_rr(r) */
 int or_vortex_line_pade(or_ctx *c, const or_line *vl, double *out);
+/* ic.f90:518-587 pade_pulse_ring: pulse != 0 for 'pulse', 0 for 'ring' */
+int or_pade_pulse_ring(or_ctx *c, int pulse, double x0, double y0, double z0, double r0, double *out);
+/* ic.f90:591-636 vortex_pair; 640-662 sphere; 666-684 sphere2; 688-709 wall */
+void or_vortex_pair(or_ctx *c, double *out);
+void or_sphere(or_ctx *c, double *out);
+void or_sphere2(or_ctx *c, double *out);
+void or_wall(or_ctx *c, double *out);
 /* complex product a*b elementwise into out (ic.in products) */
 void or_cmul(const double *a, const double *b, double *out, int64_t n);
 

@@ -81,6 +81,11 @@ def load() -> C.CDLL:
         "or_vortex_line_pade": (C.c_int, [P, C.POINTER(OrLine), P]),
         "or_fermi": (None, [P, P]),
         "or_vtrap": (None, [P, P]),
+        "or_pade_pulse_ring": (C.c_int, [P, C.c_int, D, D, D, D, P]),
+        "or_vortex_pair": (None, [P, P]),
+        "or_sphere": (None, [P, P]),
+        "or_sphere2": (None, [P, P]),
+        "or_wall": (None, [P, P]),
         "or_cmul": (None, [P, P, P, I64]),
     }
     for name, (res, args) in sig.items():
@@ -195,6 +200,31 @@ class Oracle:
         out = np.empty(self.shape, np.complex128)
         self.lib.or_fermi(self.ctx, out.ctypes.data)
         return out
+
+    def pade_pulse_ring(self, pulse_or_ring="pulse", x0=0.0, y0=0.0, z0=0.0, r0=0.0):
+        if pulse_or_ring not in ("pulse", "ring"):
+            raise ValueError("pulse_or_ring must be 'pulse' or 'ring'")
+        out = np.empty(self.shape, np.complex128)
+        self.lib.or_pade_pulse_ring(self.ctx, 1 if pulse_or_ring == "pulse" else 0, float(x0), float(y0), float(z0),
+                                    float(r0), out.ctypes.data)
+        return out
+
+    def _fill(self, fn):
+        out = np.empty(self.shape, np.complex128)
+        fn(self.ctx, out.ctypes.data)
+        return out
+
+    def vortex_pair(self):
+        return self._fill(self.lib.or_vortex_pair)
+
+    def sphere(self):
+        return self._fill(self.lib.or_sphere)
+
+    def sphere2(self):
+        return self._fill(self.lib.or_sphere2)
+
+    def wall(self):
+        return self._fill(self.lib.or_wall)
 
     def vtrap(self):
         out = np.empty(self.shape, np.float64)

@@ -46,6 +46,31 @@ def test_ic_products_and_single_precision(ring_dir):
     assert p["pr"] == 4 and p["nic"] == 2 and p["ic"][:2] == [1, 2] and p["line_dir"] == "z"
 
 
+def test_pade_pulse_and_closed_form_factors(ring_dir):
+    # pade_pulse_ring, vortex_pair, sphere, sphere2 and wall (src/ic.f90:518-709)
+    (ring_dir / "ic.in").write_text("! Pade rarefaction pulse\n"
+                                    "  init_cond = pade_pulse_ring('pulse', 0.5_pr, -1.0_pr, 2.0_pr, 0.0_pr) * "
+                                    "vortex_pair() * wall()\n")
+    p = json.loads(run_host(ring_dir, "--parse-only").stdout)
+    assert p["nic"] == 3 and p["ic"][:3] == [6, 8, 11] and p["pulse"] == [0.5, -1.0, 2.0, 0.0]
+    (ring_dir / "ic.in").write_text("  init_cond = pade_pulse_ring('ring', 0.0, 0.0, 0.0, 6.5) * sphere2() * sphere()\n")
+    p = json.loads(run_host(ring_dir, "--parse-only").stdout)
+    assert p["nic"] == 3 and p["ic"][:3] == [7, 10, 9] and p["pulse"] == [0.0, 0.0, 0.0, 6.5]
+
+
+@pytest.mark.parametrize("expr, msg", [
+    ("pade_pulse_ring('wave', 0.0, 0.0, 0.0, 1.0)", "pulse_or_ring must be 'pulse' or 'ring'"),
+    ("pade_pulse_ring('pulse', 0.0, 0.0, 1.0)", "pade_pulse_ring takes (pulse_or_ring, x0, y0, z0, r0)"),
+    ("pade_pulse_ring('pulse', 0, 0, 0, 1) * pade_pulse_ring('ring', 0, 0, 0, 2)", "different arguments"),
+    ("vortex_sheet()", "is not supported"),
+])
+def test_bad_ic_products_are_emergency_stops(ring_dir, expr, msg):
+    (ring_dir / "ic.in").write_text(f"  init_cond = {expr}\n")
+    r = run_host(ring_dir, "--parse-only")
+    assert r.returncode != 0
+    assert msg in (ring_dir / "ERROR").read_text()
+
+
 def test_unknown_scheme_is_an_emergency_stop(ring_dir):
     t = (ring_dir / "run.in").read_text().replace("'rk4'", "'rk9'")
     (ring_dir / "run.in").write_text(t)

@@ -250,6 +250,52 @@ def test_product_line_ics_match_oracle(dirn):
     np.testing.assert_allclose(o.fermi(), ic.fermi(rp), atol=1e-13)
 
 
+@pytest.mark.parametrize("kind", ["pulse", "ring"])
+def test_pade_pulse_ring_ic(kind):
+    # pade_pulse_ring (src/ic.f90:518-587): the oracle and the host
+    # restatement agree; known answers of the closed form: psi = 1 where
+    # x = x0 and s = r0 (the numerators carry the factor x2 + (1 - 2U^2) s2),
+    # psi(x0 - d) = conj(psi(x0 + d)) (uu even and vv odd in x - x0), and
+    # psi -> 1 far from the centre (along the axis vv -> -m/x^2 from above).
+    rp = RunParams(nx=21, ny=21, nz=41, xr=10.0, yr=10.0, zr=20.0)  # unit spacing: x = 0 and s = 2 are nodes
+    o = Oracle(rp)
+    a = o.pade_pulse_ring(kind, 0.0, 0.0, 0.0, 2.0 if kind == "ring" else 0.0)
+    b = ic.pade_pulse_ring(rp, kind, 0.0, 0.0, 0.0, 2.0 if kind == "ring" else 0.0)
+    np.testing.assert_allclose(a, b, rtol=0, atol=1e-14)
+    j0 = 10 + (2 if kind == "ring" else 0)
+    assert a[20, j0, 10] == 1.0 + 0.0j  # (x, y, z) = (0, s, 0) with s = r0
+    np.testing.assert_allclose(a[:, :, ::-1], np.conj(a), rtol=0, atol=1e-15)
+    m = 8.37 if kind == "pulse" else 8.97
+    far = o.pade_pulse_ring(kind, -40.0, 0.0, 0.0, 0.0)[20, 10, 20]  # on the axis, 40 from the centre
+    assert abs(far - 1.0) < 1e-2 and -m / 40.0 ** 2 < far.imag < -0.5 * m / 40.0 ** 2
+    # off-centre arguments through both restatements
+    kw = dict(x0=0.7, y0=-1.3, z0=2.1, r0=3.5)
+    np.testing.assert_allclose(o.pade_pulse_ring(kind, **kw), ic.pade_pulse_ring(rp, kind, **kw), rtol=0, atol=1e-14)
+
+
+def test_pair_sphere_wall_ics():
+    # vortex_pair (src/ic.f90:591-636), sphere (:640-662), sphere2 (:666-684)
+    # and wall (:688-709): oracle against the host restatement, and the
+    # closed forms' known values.
+    rp = RunParams(nx=21, ny=17, nz=81, xr=10.0, yr=8.0, zr=40.0)
+    o = Oracle(rp)
+    pair = o.vortex_pair()
+    np.testing.assert_allclose(pair, ic.vortex_pair(rp), rtol=0, atol=1e-14)
+    assert np.array_equal(pair, np.broadcast_to(pair[:1], pair.shape))  # the same in every z plane
+    assert pair[0, 8, 10] == pytest.approx(1.0 - 1.14026, abs=1e-15)  # x = y = 0: 1 + a0, v = 0
+    np.testing.assert_allclose(pair[:, :, ::-1], np.conj(pair), rtol=0, atol=1e-15)
+    sph = o.sphere()
+    np.testing.assert_allclose(sph, ic.sphere(rp), rtol=0, atol=1e-14)
+    assert sph[40, 8, 10].real == pytest.approx(0.5 * (1.0 + np.tanh(-12.0)), rel=1e-14)
+    sph2 = o.sphere2()
+    np.testing.assert_allclose(sph2, ic.sphere2(rp), rtol=1e-14, atol=0)
+    assert sph2[40, 8, 10] == 100.0
+    w = o.wall()
+    np.testing.assert_array_equal(w, ic.wall(rp))
+    zc = np.linspace(-40.0, 40.0, 81)
+    np.testing.assert_array_equal(w[:, 0, 0].real, np.where(zc <= -30.0, 0.0, 1.0))
+
+
 def test_golden_oracle_regression():
     """The oracle still reproduces its committed small-grid runs bit for bit."""
     from tests.golden.make_golden import CASES, SHAPE
