@@ -221,6 +221,30 @@ RunIn parse_run_in() {
   lg(io, "save_spectrum", r.save_spectrum);
   lg(io, "save_filter", r.save_filter);
   num(io, "filter_kc", r.filter_kc);
+  // diagnostics of the reference loop this host does not write
+  // (src/gpe.f90:98, 181-217, 237-239): a run that asks for one stops with
+  // ERROR instead of silently producing fewer files
+  const std::pair<const char*, const char*> unbuilt[] = {
+      {"save_contour", "save_surface (src/io.f90:440-476)"},
+      {"save_average", "average (src/io.f90:1470-1500)"},
+      {"save_pdf", "save_velocity_pdf (src/io.f90:211-274)"},
+      {"save_vcf", "save_vel_corr (src/io.f90:278-300)"},
+      {"save_ll", "save_linelength (src/io.f90:1397-1429)"},
+      {"save_zeros", "get_zeros/get_extra_zeros/get_re_im_zeros (src/io.f90:886-1393)"}};
+  for (const auto& u : unbuilt) {
+    bool on = false;
+    lg(io, u.first, on);
+    if (on) emergency_stop(std::string("ERROR: ") + u.first + " = .true. needs " + u.second + ", which this host does not write.");
+  }
+  auto& mp = nl["misc_params"];
+  bool on = false;
+  lg(mp, "diagnostic", on);
+  if (on) emergency_stop("ERROR: diagnostic = .true. needs diag (src/io.f90:1433-1466), which this host does not write.");
+  on = false;
+  lg(mp, "pp_filtered_surface", on);
+  if (on)
+    emergency_stop("ERROR: pp_filtered_surface = .true. needs pp_save_filter (src/io.f90:1504-1554), which this host "
+                   "does not run.");
   return r;
 }
 

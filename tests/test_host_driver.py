@@ -71,6 +71,22 @@ def test_bad_ic_products_are_emergency_stops(ring_dir, expr, msg):
     assert msg in (ring_dir / "ERROR").read_text()
 
 
+@pytest.mark.parametrize("group, flag", [("io_params", "save_contour"), ("io_params", "save_average"),
+                                         ("io_params", "save_pdf"), ("io_params", "save_vcf"),
+                                         ("io_params", "save_ll"), ("io_params", "save_zeros"),
+                                         ("misc_params", "diagnostic"), ("misc_params", "pp_filtered_surface")])
+def test_unbuilt_diagnostics_are_emergency_stops(ring_dir, group, flag):
+    # a run that asks for a diagnostic this host does not write stops with
+    # ERROR (src/error.f90:24-46) instead of silently writing fewer files
+    t = (ring_dir / "run.in").read_text()
+    t = t.replace(f"  {flag}  = .false.\n", "")
+    head = t.index(f"&{group}") + len(f"&{group}") + 1
+    (ring_dir / "run.in").write_text(t[:head] + f"  {flag} = .true.\n" + t[head:])
+    r = run_host(ring_dir, "--parse-only")
+    assert r.returncode != 0
+    assert f"{flag} = .true. needs" in (ring_dir / "ERROR").read_text()
+
+
 def test_unknown_scheme_is_an_emergency_stop(ring_dir):
     t = (ring_dir / "run.in").read_text().replace("'rk4'", "'rk9'")
     (ring_dir / "run.in").write_text(t)
