@@ -28,12 +28,9 @@
 #include "gpe_ic.h"
 
 namespace gpe {
-cudaError_t launch_batch_f64(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                             const int* order, int nitems, int* queue, double* partials, int* occupancy);
-cudaError_t launch_batch_f32(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                             const int* order, int nitems, int* queue, double* partials, int* occupancy);
-cudaError_t launch_batch_f32x(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                              const int* order, int nitems, int* queue, double* partials, int* occupancy);
+cudaError_t launch_batch_f64(int kind, int R, int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy);
+cudaError_t launch_batch_f32(int kind, int R, int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy);
+cudaError_t launch_batch_f32x(int kind, int R, int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy);
 int batch_rows_f64(int kind);
 int batch_rows_f32(int kind);
 int batch_rows_f32x(int kind);
@@ -239,14 +236,12 @@ int cmode_of(const gpe_params& p) {
   return p.compute == GPE_COMPUTE_F64 ? CM_F32X : CM_F32;
 }
 
-cudaError_t launch_batch(int cls, int kind, int grid, cudaStream_t st, const BatchStage* tab,
-                         const BatchItem* items, const int* order, int nitems, int* queue, double* partials,
-                         int* occ) {
+cudaError_t launch_batch(int cls, int kind, int grid, cudaStream_t st, const BatchLaunch& b, int* occ) {
   const int R = class_radius(cls);
   switch (class_cmode(cls)) {
-    case CM_F64: return launch_batch_f64(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
-    case CM_F32: return launch_batch_f32(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
-    default: return launch_batch_f32x(kind, R, grid, st, tab, items, order, nitems, queue, partials, occ);
+    case CM_F64: return launch_batch_f64(kind, R, grid, st, b, occ);
+    case CM_F32: return launch_batch_f32(kind, R, grid, st, b, occ);
+    default: return launch_batch_f32x(kind, R, grid, st, b, occ);
   }
 }
 
@@ -262,7 +257,7 @@ int batch_rows(int cmode, int fam) {
 
 int grid_for(int cls, int kind, int nitems) {
   int occ = 0;
-  launch_batch(cls, kind, 0, nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, &occ);
+  launch_batch(cls, kind, 0, nullptr, BatchLaunch{}, &occ);
   return std::max(1, std::min(nitems, occ));
 }
 
@@ -438,8 +433,10 @@ int capture_rk4_step(gpe_pool* P, Class& c, int cm, int ns, const int* grids, bo
   cudaError_t e = cudaMemsetAsync(c.queue.p, 0, 4 * sizeof(int), c.st);
   for (int m = 0; m < 4 && e == cudaSuccess; ++m) {
     const int row = (m == 3 && !with_norm) ? 4 : m;
-    e = launch_batch(cm, kinds[m], grids[m], c.st, c.tab.p + (size_t)row * ns, c.items.p, c.order.p, c.nitems,
-                     c.queue.p + m, (m == 3 && with_norm) ? c.part.p : nullptr, nullptr);
+    e = launch_batch(cm, kinds[m], grids[m], c.st,
+                     BatchLaunch{c.tab.p + (size_t)row * ns, c.htab.p + (size_t)row * ns, ns, c.items.p, c.order.p,
+                                 c.nitems, c.queue.p + m, (m == 3 && with_norm) ? c.part.p : nullptr},
+                     nullptr);
   }
   cudaGraph_t g = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(c.st, &g);
@@ -535,8 +532,10 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
   PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
   PCU(P, cudaMemsetAsync(c.queue.p, 0, 6 * sizeof(int), c.st));
   for (int m = 0; m < 6; ++m)
-    PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), c.st, c.tab.p + (size_t)m * ns,
-                        c.items.p, c.order.p, c.nitems, c.queue.p + m, m == 5 ? c.part.p : nullptr, nullptr));
+    PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), c.st,
+                        BatchLaunch{c.tab.p + (size_t)m * ns, c.htab.p + (size_t)m * ns, ns, c.items.p, c.order.p,
+                                    c.nitems, c.queue.p + m, m == 5 ? c.part.p : nullptr},
+                        nullptr));
   k_finalize_ranges<<<ns, 256, 0, c.st>>>(c.part.p, c.first.p, c.res.p);
   PCU(P, cudaGetLastError());
   PCU(P, cudaMemcpyAsync(c.hres.p, c.res.p, (size_t)ns * RED_SLOTS * sizeof(double), cudaMemcpyDeviceToHost, c.st));

@@ -4,6 +4,7 @@
 //                                  cudaStream_t st, const StageArgs& a)
 #pragma once
 #include <cstdlib>
+#include <memory>
 #include <type_traits>
 
 #include "gpe_device.cuh"
@@ -184,7 +185,7 @@ __host__ __device__ constexpr bool is_rk4_kind(int k) {
 
 // Opt the batched kernel into its dynamic shared memory once per device and
 // cache how many of its CTAs fit on the device at once.
-template <class S, class C, int K, int TY, bool PAIR, int RR>
+template <class S, class C, int K, int TY, bool PAIR, int RR, bool PARG = false>
 static cudaError_t batch_setup(int* occupancy) {
   using LY = TmaLayout<S, RR, StageTraits<K>::NPW, TY>;
   static unsigned long long done = 0;
@@ -193,12 +194,12 @@ static cudaError_t batch_setup(int* occupancy) {
   cudaGetDevice(&dev);
   if (dev >= 64) return cudaErrorInvalidDevice;
   if (!(done & (1ULL << dev))) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, PARG>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LY::SMEM);
     if (e != cudaSuccess) return e;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, PARG>,
                                                       batch_threads<TY, BATCH_PY, PAIR>(), LY::SMEM);
     if (e != cudaSuccess) return e;
     occ[dev] = nsm * (per > 0 ? per : 1);
@@ -208,55 +209,62 @@ static cudaError_t batch_setup(int* occupancy) {
   return cudaSuccess;
 }
 
+// One launch; with at most BATCH_PARAM_SOLVES solves their stage arguments
+// go into the launch's parameter space (the PARG kernel), else the kernel
+// reads them from the device table.
 template <class S, class C, int K, int TY, bool PAIR, int RR>
-static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                                    const int* order, int nitems, int* queue, double* partials) {
+static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchLaunch& b) {
   using LY = TmaLayout<S, RR, StageTraits<K>::NPW, TY>;
-  cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR>(nullptr);
-  if (e != cudaSuccess) return e;
   const dim3 block = PAIR ? dim3(16, 8) : dim3(32, TY / BATCH_PY);
-  k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR><<<grid, block, LY::SMEM, st>>>(tab, items, order, nitems, queue,
-                                                                                 partials);
+  if (b.htab && b.ns >= 1 && b.ns <= BATCH_PARAM_SOLVES) {
+    cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR, true>(nullptr);
+    if (e != cudaSuccess) return e;
+    thread_local std::unique_ptr<BatchArgs> pa;  // 32 KB staging, copied by the launch
+    if (!pa) pa.reset(new BatchArgs);
+    for (int q = 0; q < b.ns; ++q) pa->a[q] = b.htab[q].args;
+    k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, true>
+        <<<grid, block, LY::SMEM, st>>>(b.tab, b.items, b.order, b.nitems, b.queue, b.partials, *pa);
+    return cudaGetLastError();
+  }
+  cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR, false>(nullptr);
+  if (e != cudaSuccess) return e;
+  k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, false>
+      <<<grid, block, LY::SMEM, st>>>(b.tab, b.items, b.order, b.nitems, b.queue, b.partials, NoBatchArgs{});
   return cudaGetLastError();
 }
 
 template <class S, class C, int K, int RR>
-static cudaError_t launch_batch_kind_r(int grid, cudaStream_t st, const BatchStage* tab, const BatchItem* items,
-                                       const int* order, int nitems, int* queue, double* partials,
-                                       int* occupancy) {
+static cudaError_t launch_batch_kind_r(int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy) {
   if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
     if constexpr (is_rk4_kind(K)) {
       if (batch_rk4_f32_rows() == 16) {
         if (grid <= 0) return batch_setup<S, C, K, 16, true, RR>(occupancy);
-        return launch_batch_one<S, C, K, 16, true, RR>(grid, st, tab, items, order, nitems, queue, partials);
+        return launch_batch_one<S, C, K, 16, true, RR>(grid, st, b);
       }
     }
     if (batch_pair_layout()) {
       if (grid <= 0) return batch_setup<S, C, K, 8, true, RR>(occupancy);
-      return launch_batch_one<S, C, K, 8, true, RR>(grid, st, tab, items, order, nitems, queue, partials);
+      return launch_batch_one<S, C, K, 8, true, RR>(grid, st, b);
     }
   }
   if (grid <= 0) return batch_setup<S, C, K, 8, false, RR>(occupancy);
-  return launch_batch_one<S, C, K, 8, false, RR>(grid, st, tab, items, order, nitems, queue, partials);
+  return launch_batch_one<S, C, K, 8, false, RR>(grid, st, b);
 }
 
 template <class S, class C, int K>
-static cudaError_t launch_batch_kind(int R, int grid, cudaStream_t st, const BatchStage* tab,
-                                     const BatchItem* items, const int* order, int nitems, int* queue,
-                                     double* partials, int* occupancy) {
-  if (R == 1) return launch_batch_kind_r<S, C, K, 1>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
-  if (R == 2) return launch_batch_kind_r<S, C, K, 2>(grid, st, tab, items, order, nitems, queue, partials, occupancy);
+static cudaError_t launch_batch_kind(int R, int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy) {
+  if (R == 1) return launch_batch_kind_r<S, C, K, 1>(grid, st, b, occupancy);
+  if (R == 2) return launch_batch_kind_r<S, C, K, 2>(grid, st, b, occupancy);
   return cudaErrorInvalidValue;
 }
 
 template <class S, class C>
-static cudaError_t launch_batch_impl(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab,
-                                     const BatchItem* items, const int* order, int nitems, int* queue,
-                                     double* partials, int* occupancy) {
+static cudaError_t launch_batch_impl(int kind, int R, int grid, cudaStream_t st, const BatchLaunch& b,
+                                     int* occupancy) {
   switch (kind) {
 #define GPE_BCASE(K) \
   case K:            \
-    return launch_batch_kind<S, C, K>(R, grid, st, tab, items, order, nitems, queue, partials, occupancy);
+    return launch_batch_kind<S, C, K>(R, grid, st, b, occupancy);
     GPE_BCASE(K_RK4_1)
     GPE_BCASE(K_RK4_2)
     GPE_BCASE(K_RK4_3)
@@ -297,10 +305,8 @@ static cudaError_t launch_stage_impl(int kind, int R, int ty, dim3 grid, cudaStr
                ? batch_rk4_f32_rows()                                                                    \
                : 8;                                                                                      \
   }                                                                                                       \
-  cudaError_t launch_batch_##TAG(int kind, int R, int grid, cudaStream_t st, const BatchStage* tab,     \
-                                 const BatchItem* items, const int* order, int nitems, int* queue,     \
-                                 double* partials, int* occupancy) {                                   \
-    return launch_batch_impl<S, C>(kind, R, grid, st, tab, items, order, nitems, queue, partials,       \
-                                   occupancy);                                                          \
+  cudaError_t launch_batch_##TAG(int kind, int R, int grid, cudaStream_t st, const BatchLaunch& b,      \
+                                 int* occupancy) {                                                     \
+    return launch_batch_impl<S, C>(kind, R, grid, st, b, occupancy);                                    \
   }                                                                                                     \
   }

@@ -18,6 +18,8 @@
 #pragma once
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "gpe_device.cuh"
 
 namespace gpe {
@@ -719,6 +721,36 @@ struct BatchItem {
   int solve, bx, by, bz;
 };
 
+// The per-solve stage arguments of one batched launch as a kernel parameter
+// (32 KB of parameter space, read through the constant cache): up to
+// BATCH_PARAM_SOLVES solves.  Items index it by their solve, and the item
+// body reads its arguments from there as the single-solve kernels read
+// theirs.  Loaded per item from the global table into registers instead,
+// they keep the kernel at its 128-register bound, and the stages of one
+// 256^3 solve in a pool take 6-8 % longer (a launch with more solves keeps
+// that path).
+constexpr int BATCH_PARAM_SOLVES = 72;
+struct BatchArgs {
+  StageArgs a[BATCH_PARAM_SOLVES];
+};
+struct NoBatchArgs {};
+static_assert(sizeof(BatchArgs) + 256 <= 32764, "batched launch parameters exceed the 32 KB parameter space");
+template <bool PARG>
+using BatchArgsOf = typename std::conditional<PARG, BatchArgs, NoBatchArgs>::type;
+
+// One batched launch: tab = the device rows of the ns solves (stage
+// arguments + tensor maps), htab = the same rows on the host.
+struct BatchLaunch {
+  const BatchStage* tab;
+  const BatchStage* htab;
+  int ns;
+  const BatchItem* items;
+  const int* order;
+  int nitems;
+  int* queue;
+  double* partials;
+};
+
 // CTAs per SM the batched kernels' registers are fitted to.  The R = 1 and
 // R = 2 item bodies share one kernel, so unbounded they take 96-128
 // registers (RK4) and 136-185 (Cash-Karp) at FP32, 124-154 and 190-229 at
@@ -750,10 +782,11 @@ __host__ __device__ constexpr int batch_threads() {
 // the stencil radius of every solve the launch serves (a pool keeps solves
 // of the two FD orders in separate classes): one item body per kernel, and
 // rings sized for that radius.
-template <class S, class C, int KIND, int TY, int PY, bool PAIR, int RR>
+template <class S, class C, int KIND, int TY, int PY, bool PAIR, int RR, bool PARG>
 __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_blocks<C, KIND, PAIR ? TY : 8>()))
     k_stage_batch(const BatchStage* __restrict__ tab, const BatchItem* __restrict__ items,
-                  const int* __restrict__ order, int nitems, int* queue, double* partials) {
+                  const int* __restrict__ order, int nitems, int* queue, double* partials,
+                  const __grid_constant__ BatchArgsOf<PARG> pa) {
   static_assert(!PAIR || (sizeof(S) == 8 && sizeof(C) == 4 && (TY == 8 || TY == 16)),
                 "the pair layout is for complex64 / FP32 on 32 x 8 or 32 x 16 items");
   static_assert(RR == 1 || RR == 2, "stencil radius 1 or 2");
@@ -781,18 +814,25 @@ __global__ void __launch_bounds__(batch_threads<TY, PY, PAIR>(), (batch_min_bloc
       for (int f = 0; f < StageTraits<KIND>::NPW; ++f) tensormap_acquire(&bs->maps.pw[f]);
       fenced = it.solve;
     }
-    // the item's arguments in registers (read-only path, same address for
-    // every thread); a shared-memory copy would be re-read after every
-    // barrier of the z march
-    const StageArgs sa = __ldg_args(&bs->args);
     double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
+    auto run = [&](const StageArgs& sa) {
+      if constexpr (PAIR)
+        return tma_item_pair<C, RR, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm,
+                                                       r_en, r_err);
+      else
+        return tma_item<S, C, RR, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
+                                                    r_err);
+    };
     bool ok;
-    if constexpr (PAIR)
-      ok = tma_item_pair<C, RR, KIND, TY, PYP, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                   r_err);
-    else
-      ok = tma_item<S, C, RR, KIND, TY, PY, LY>(bs->maps, sa, it.bx, it.by, it.bz, rg, &s_abort, r_norm, r_en,
-                                                r_err);
+    if constexpr (PARG) {
+      ok = run(pa.a[it.solve]);  // parameter space: the host puts at most BATCH_PARAM_SOLVES rows there
+    } else {
+      // the item's arguments in registers (read-only path, same address for
+      // every thread); a shared-memory copy would be re-read after every
+      // barrier of the z march
+      const StageArgs sa = __ldg_args(&bs->args);
+      ok = run(sa);
+    }
     if (!ok) return;
     if (partials) block_reduce_store_at<NT>(r_norm, r_en, r_err, partials, w);
   }
