@@ -751,16 +751,12 @@ struct BatchLaunch {
   double* partials;
 };
 
-// CTAs per SM the batched kernels' registers are fitted to.  The R = 1 and
-// R = 2 item bodies share one kernel, so unbounded they take 96-128
-// registers (RK4) and 136-185 (Cash-Karp) at FP32, 124-154 and 190-229 at
-// FP64.  Bounded, they spill at most a few words: RK4 to 6 CTAs of 128
-// threads at FP32 (80 registers) and 4 at FP64 (+2-4 % on a batch of uneven
-// solves); Cash-Karp to 4 at FP32 (+8 % on a batch of RKF45 solves) and 3
-// at FP64 (neutral; stages 3-6 are held to 2 CTAs by shared memory anyway).
-// The complex64 pair layout on 32 x 16 items (four sites per thread) holds
-// twice the sites per thread and is fitted to 4 CTAs, as its single-solve
-// form.
+// CTAs per SM the batched kernels' registers are fitted to (each kernel
+// carries the item body of one stencil radius).  RK4: 4 CTAs of 128 threads
+// for the complex64 pair layout on 32 x 16 items (four sites per thread, as
+// its single-solve form) and at FP64, 6 for FP32 on 32 x 8 items;
+// Cash-Karp: 4 at FP32 (+8 % against unbounded on a batch of RKF45 solves)
+// and 3 at FP64 (stages 3-6 are held to 2 CTAs by shared memory anyway).
 template <class C, int KIND, int TY = 8>
 __host__ __device__ constexpr int batch_min_blocks() {
   return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4)
