@@ -241,23 +241,32 @@ def test_fp32_storage_trapped_vs_fp64_oracle(gpu):
     assert drift <= 1e-7
 
 
-@pytest.mark.slow
-def test_fp32_storage_c2_256_cubed_vs_oracle(gpu):
+C2_RP = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
+                  eqn_to_solve=2, bcs=1, order=4)
+
+
+@pytest.fixture(scope="module")
+def c2_oracle_200():
     """The roofline workload (256^3 random phase, periodic, 4th order, RK4
-    dt = 0.005, eqn 2) in complex64 storage with the FP32 stencil, 200 steps,
-    against the FP64 CPU oracle on the same initial state."""
-    rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
-                   eqn_to_solve=2, bcs=1, order=4)
-    psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
-    s = Solver(rp.replace(storage="c64", compute="f32"))
+    dt = 0.005, eqn 2) run 200 steps by the FP64 CPU oracle, once for the
+    tests of this module: (psi0, psi_200, norm, energy)."""
+    psi0 = ic.random_phase(C2_RP, seed=1234, kc=1.5)
+    o = Oracle(C2_RP)
+    ref = o.run(psi0, 200)
+    return psi0, ref, o.get_norm(ref), o.energy(ref)
+
+
+@pytest.mark.slow
+def test_fp32_storage_c2_256_cubed_vs_oracle(gpu, c2_oracle_200):
+    """The roofline workload in complex64 storage with the FP32 stencil, 200
+    steps, against the FP64 CPU oracle on the same initial state."""
+    psi0, ref, nref, eref = c2_oracle_200
+    s = Solver(C2_RP.replace(storage="c64", compute="f32"))
     s.set_state(psi0)
     s.solver(200)
     out = s.get_state()
     n32, e32 = s.get_norm(), s.energy()
     s.close()
-    o = Oracle(rp)
-    ref = o.run(psi0, 200)
-    nref, eref = o.get_norm(ref), o.energy(ref)
     err = rel_l2(out, ref)
     drift = abs(n32 - nref) / nref
     edrift = abs(e32 - eref) / abs(eref)
@@ -309,13 +318,19 @@ def test_fp32_storage_rk45_trapped_vs_fp64_oracle(gpu):
 
 
 @pytest.mark.slow
-def test_c2_256_cubed_periodic_o4(gpu):
-    rp = RunParams(nx=256, ny=256, nz=256, xr=63.75, yr=63.75, zr=63.75, tau=0.005, scheme="rk4",
-                   eqn_to_solve=2, bcs=1, order=4)
-    psi0 = ic.random_phase(rp, seed=1234, kc=1.5)
-    o, ref, s, out, info = run_both(rp, psi0, 4, want_norm=True)
+def test_c2_256_cubed_periodic_o4(gpu, c2_oracle_200):
+    """The roofline workload in complex128, 200 steps through the replayed
+    step graph, against the FP64 CPU oracle: psi, norm and energy."""
+    psi0, ref, nref, eref = c2_oracle_200
+    s = Solver(C2_RP)
+    s.set_state(psi0)
+    info = s.solver(200, want_norm=True)
+    out = s.get_state()
+    e = s.energy()
+    s.close()
     assert rel_l2(out, ref) <= TOL64
-    assert info.norm == pytest.approx(o.get_norm(ref), rel=TOL64)
+    assert info.norm == pytest.approx(nref, rel=TOL64)
+    assert e == pytest.approx(eref, rel=TOL64)
 
 
 def test_snapshot_while_stepping(gpu):
