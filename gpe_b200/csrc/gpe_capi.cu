@@ -173,6 +173,7 @@ int field_of(const gpe_handle* h, const void* p) {
 cudaError_t launch_raw(gpe_handle* h, int kind, const StageArgs& a_in) {
   StageArgs a = a_in;
   a.status = h->status;
+  set_f32_constants(a);
   if (!h->use_tma) {
     switch (h->cmode) {
       case CM_F64: return launch_stage_f64(kind, h->R, 8, h->grid, h->st, a);

@@ -95,7 +95,43 @@ struct alignas(16) StageArgs {
   int* status;                  // device status word: non-zero = a bounded wait expired
   int zghost;                   // z ghosts the producer writes: bit 0 below the grid, bit 1 above
   int eqn4_plain;               // eqn 4 with V = 0 and gamma = 0 (the trap and damping terms vanish)
+  // The FP32 stencil's copies of the constants above, each the double
+  // rounded once to float on the host (set_f32_constants), so that the
+  // kernels convert nothing per site or per plane
+  float f_ixx, f_iyy, f_izz, f_ix1;
+  float f_g_nl, f_mu, f_gamma, f_urhs, f_diss_amp;
+  float f_cf_r[2], f_cf_i[2];
+  float f_b[6];
+  float f_pad;
 };
+
+// The stencil's compute-type copy of a stage constant: the float copy for
+// the FP32 stencil, the double itself for FP64.
+template <class C>
+__host__ __device__ __forceinline__ C cval(double d, float f) {
+  if constexpr (sizeof(C) == sizeof(float)) return f;
+  else return (C)d;
+}
+
+// Fill the float copies of a's constants (round to nearest, as the device's
+// (float) conversion of the same double).
+inline void set_f32_constants(StageArgs& a) {
+  a.f_ixx = (float)a.ixx;
+  a.f_iyy = (float)a.iyy;
+  a.f_izz = (float)a.izz;
+  a.f_ix1 = (float)a.ix1;
+  a.f_g_nl = (float)a.g_nl;
+  a.f_mu = (float)a.mu;
+  a.f_gamma = (float)a.gamma;
+  a.f_urhs = (float)a.urhs;
+  a.f_diss_amp = (float)a.diss_amp;
+  for (int q = 0; q < 2; ++q) {
+    a.f_cf_r[q] = (float)a.cf_r[q];
+    a.f_cf_i[q] = (float)a.cf_i[q];
+  }
+  for (int q = 0; q < 6; ++q) a.f_b[q] = (float)a.b[q];
+  a.f_pad = 0.0f;
+}
 
 static_assert(sizeof(StageArgs) % 16 == 0, "StageArgs is copied in 16-byte words");
 
@@ -338,7 +374,7 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
     // FP64 as 0.5 ((vx + vy) + vz); in FP32 compute as the sum of the
     // column's and the plane's halves, each rounded once to float (no FP64
     // operations or conversions per site)
-    const C g = (C)a.g_nl, mu = (C)a.mu, gm = (C)a.gamma;
+    const C g = cval<C>(a.g_nl, a.f_g_nl), mu = cval<C>(a.mu, a.f_mu), gm = cval<C>(a.gamma, a.f_gamma);
     if (a.eqn4_plain) {
       // V = 0, gamma = 0: the same sums without their zero terms (the
       // results agree bit for bit up to the sign of a zero)
@@ -372,7 +408,7 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
       r[q].i = cr;
     }
     if (a.has_urhs) {
-      const C u = (C)a.urhs;
+      const C u = cval<C>(a.urhs, a.f_urhs);
 #pragma unroll
       for (int q = 0; q < PY; ++q) {
         r[q].r += u * dpx[q].r;
@@ -390,7 +426,7 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
 #pragma unroll
         for (int q = 0; q < PY; ++q) dd[q] = 0.5 * (a.diss_amp * (cc[q].sxy + sz));
       } else {
-        const C amp = (C)a.diss_amp, szf = (C)sz;
+        const C amp = cval<C>(a.diss_amp, a.f_diss_amp), szf = (C)sz;
 #pragma unroll
         for (int q = 0; q < PY; ++q) dd[q] = (C)0.5 * (amp * (cc[q].sxy + szf));
       }
@@ -403,7 +439,7 @@ __device__ __forceinline__ void gp_rhs_n(const StageArgs& a, const cx<C> (&p)[PY
       r[q].i = dd[q] * ci + (C)0.5 * cr;
     }
     if (a.has_urhs) {
-      const C u = (C)a.urhs;
+      const C u = cval<C>(a.urhs, a.f_urhs);
 #pragma unroll
       for (int q = 0; q < PY; ++q) {
         r[q].r += u * dpx[q].r;
@@ -439,13 +475,13 @@ template <class C, int R>
 __device__ __forceinline__ cx<C> site_lap(const StageArgs& a, const Nb<C>& b) {
   cx<C> lap;
   if constexpr (sizeof(C) == sizeof(double)) {
-    const cx<C> lxx = d2<C, R>(b.xm2, b.xm1, b.c0, b.xp1, b.xp2, (C)a.ixx);
-    const cx<C> lyy = d2<C, R>(b.ym2, b.ym1, b.c0, b.yp1, b.yp2, (C)a.iyy);
-    const cx<C> lzz = d2<C, R>(b.zm2, b.zm1, b.c0, b.zp1, b.zp2, (C)a.izz);
+    const cx<C> lxx = d2<C, R>(b.xm2, b.xm1, b.c0, b.xp1, b.xp2, cval<C>(a.ixx, a.f_ixx));
+    const cx<C> lyy = d2<C, R>(b.ym2, b.ym1, b.c0, b.yp1, b.yp2, cval<C>(a.iyy, a.f_iyy));
+    const cx<C> lzz = d2<C, R>(b.zm2, b.zm1, b.c0, b.zp1, b.zp2, cval<C>(a.izz, a.f_izz));
     lap.r = (lxx.r + lyy.r) + lzz.r;
     lap.i = (lxx.i + lyy.i) + lzz.i;
   } else {
-    const C ix = (C)a.ixx, iy = (C)a.iyy, iz = (C)a.izz;
+    const C ix = cval<C>(a.ixx, a.f_ixx), iy = cval<C>(a.iyy, a.f_iyy), iz = cval<C>(a.izz, a.f_izz);
     auto axis = [](C m2, C m1, C c, C p1, C p2) -> C {
       if constexpr (R == 1) return (p1 - (C)2 * c) + m1;
       else return ((((-p2 + (C)16 * p1) - (C)30 * c) + (C)16 * m1) - m2);
@@ -465,7 +501,7 @@ __device__ __forceinline__ cx<C> site_lap(const StageArgs& a, const Nb<C>& b) {
 // First x-derivative of one site (only read when Urhs != 0).
 template <class C, int R>
 __device__ __forceinline__ cx<C> site_dpx(const StageArgs& a, const Nb<C>& b) {
-  return d1<C, R>(b.xm2, b.xm1, b.xp1, b.xp2, (C)a.ix1);
+  return d1<C, R>(b.xm2, b.xm1, b.xp1, b.xp2, cval<C>(a.ix1, a.f_ix1));
 }
 
 // Everything a stage does at the PY interior sites (i, j_q, k) of one thread
@@ -551,7 +587,7 @@ __device__ __forceinline__ void sites_update(const StageArgs& a, const cx<C> (&l
           ns[q] = to_s<S>(cx<double>{base.r + t0.r, base.i + t0.i});
         } else {
           const cx<C> base = (KIND == K_RK2_2 || KIND == K_RK4_2 || KIND == K_RK4_3) ? to_c<C>(pv) : c0[q];
-          const C ar = (C)a.cf_r[0], ai = (C)a.cf_i[0];
+          const C ar = cval<C>(a.cf_r[0], a.f_cf_r[0]), ai = cval<C>(a.cf_i[0], a.f_cf_i[0]);
           ns[q] = to_s<S>(cx<C>{base.r + (ar * f[q].r - ai * f[q].i), base.i + (ar * f[q].i + ai * f[q].r)});
         }
         if constexpr (MAIN) {
@@ -568,7 +604,7 @@ __device__ __forceinline__ void sites_update(const StageArgs& a, const cx<C> (&l
             qs = to_s<S>(cx<double>{(pd.r + cr) + t1.r, (pd.i + ci) + t1.i});
           } else {
             const cx<C> pc = to_c<C>(pv);
-            const C br = (C)a.cf_r[1], bi = (C)a.cf_i[1];
+            const C br = cval<C>(a.cf_r[1], a.f_cf_r[1]), bi = cval<C>(a.cf_i[1], a.f_cf_i[1]);
             qs = to_s<S>(cx<C>{(pc.r + c0[q].r) + (br * f[q].r - bi * f[q].i),
                                (pc.i + c0[q].i) + (br * f[q].i + bi * f[q].r)});
           }
@@ -581,8 +617,8 @@ __device__ __forceinline__ void sites_update(const StageArgs& a, const cx<C> (&l
       } else if constexpr (KIND != K_CK_6 && sizeof(C) != sizeof(double)) {
         // Cash-Karp stages 1-5 in the stencil's compute type: K_m = dt f and
         // tmp = psi + sum_j b_j K_j feed the next stencil only
-        const cx<C> Km{(C)a.cf_r[0] * f[q].r - (C)a.cf_i[0] * f[q].i,
-                       (C)a.cf_r[0] * f[q].i + (C)a.cf_i[0] * f[q].r};
+        const C kr = cval<C>(a.cf_r[0], a.f_cf_r[0]), ki = cval<C>(a.cf_i[0], a.f_cf_i[0]);
+        const cx<C> Km{kr * f[q].r - ki * f[q].i, kr * f[q].i + ki * f[q].r};
         const S Ks = to_s<S>(Km);
         if constexpr (MAIN) {
           if (act[q]) ((S*)a.kout)[o[q]] = Ks;
@@ -595,11 +631,11 @@ __device__ __forceinline__ void sites_update(const StageArgs& a, const cx<C> (&l
 #pragma unroll
         for (int m = 0; m < T::NK; ++m) {
           const cx<C> km = to_c<C>(pw[q][K0 + m]);
-          tr = tr + (C)a.b[m] * km.r;
-          ti = ti + (C)a.b[m] * km.i;
+          tr = tr + cval<C>(a.b[m], a.f_b[m]) * km.r;
+          ti = ti + cval<C>(a.b[m], a.f_b[m]) * km.i;
         }
-        tr = tr + (C)a.b[T::NK] * Kmc.r;
-        ti = ti + (C)a.b[T::NK] * Kmc.i;
+        tr = tr + cval<C>(a.b[T::NK], a.f_b[T::NK]) * Kmc.r;
+        ti = ti + cval<C>(a.b[T::NK], a.f_b[T::NK]) * Kmc.i;
         ns[q] = to_s<S>(cx<C>{tr, ti});
         if constexpr (MAIN) {
           if (act[q]) store_at<GXY, GZ>(out, g, o[q], i, j[q], k, cc[q].gx, cc[q].gy, gz, ns[q]);

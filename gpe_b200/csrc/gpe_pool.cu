@@ -473,6 +473,7 @@ int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
       b.args.want_norm = 0;
       c.htab.p[(size_t)4 * ns + q] = b;
     }
+    for (size_t r = 0; r < (size_t)5 * ns; ++r) set_f32_constants(c.htab.p[r].args);
     PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)5 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
     const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_3, K_RK4_4};
     int grids[4];
@@ -529,6 +530,7 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
     rk45_tables(P, sv[q], t6.data());
     for (int m = 0; m < 6; ++m) c.htab.p[(size_t)m * ns + q] = t6[m];
   }
+  for (size_t r = 0; r < (size_t)6 * ns; ++r) set_f32_constants(c.htab.p[r].args);
   PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
   PCU(P, cudaMemsetAsync(c.queue.p, 0, 6 * sizeof(int), c.st));
   for (int m = 0; m < 6; ++m)

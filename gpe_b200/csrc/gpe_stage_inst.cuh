@@ -211,20 +211,27 @@ static cudaError_t batch_setup(int* occupancy) {
 
 // One launch; with at most BATCH_PARAM_SOLVES solves their stage arguments
 // go into the launch's parameter space (the PARG kernel), else the kernel
-// reads them from the device table.
+// reads them from the device table.  FP32 Cash-Karp stages keep the table
+// path: their item bodies read the arguments so often per site that
+// constant-cache reads cost more than the registers they free (a batch of
+// 16 FP32 RKF45 solves: 9.8 against 10.5 G accepted site-updates/s; FP64
+// Cash-Karp gains 14 %, the RK4 stages 4 %).
 template <class S, class C, int K, int TY, bool PAIR, int RR>
 static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchLaunch& b) {
   using LY = TmaLayout<S, RR, StageTraits<K>::NPW, TY>;
   const dim3 block = PAIR ? dim3(16, 8) : dim3(32, TY / BATCH_PY);
-  if (b.htab && b.ns >= 1 && b.ns <= BATCH_PARAM_SOLVES) {
-    cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR, true>(nullptr);
-    if (e != cudaSuccess) return e;
-    thread_local std::unique_ptr<BatchArgs> pa;  // 32 KB staging, copied by the launch
-    if (!pa) pa.reset(new BatchArgs);
-    for (int q = 0; q < b.ns; ++q) pa->a[q] = b.htab[q].args;
-    k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, true>
-        <<<grid, block, LY::SMEM, st>>>(b.tab, b.items, b.order, b.nitems, b.queue, b.partials, *pa);
-    return cudaGetLastError();
+  constexpr bool kParamArgs = !(sizeof(C) == sizeof(float) && K >= K_CK_1 && K <= K_CK_6);
+  if constexpr (kParamArgs) {
+    if (b.htab && b.ns >= 1 && b.ns <= BATCH_PARAM_SOLVES) {
+      cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR, true>(nullptr);
+      if (e != cudaSuccess) return e;
+      thread_local std::unique_ptr<BatchArgs> pa;  // 32 KB staging, copied by the launch
+      if (!pa) pa.reset(new BatchArgs);
+      for (int q = 0; q < b.ns; ++q) pa->a[q] = b.htab[q].args;
+      k_stage_batch<S, C, K, TY, BATCH_PY, PAIR, RR, true>
+          <<<grid, block, LY::SMEM, st>>>(b.tab, b.items, b.order, b.nitems, b.queue, b.partials, *pa);
+      return cudaGetLastError();
+    }
   }
   cudaError_t e = batch_setup<S, C, K, TY, PAIR, RR, false>(nullptr);
   if (e != cudaSuccess) return e;

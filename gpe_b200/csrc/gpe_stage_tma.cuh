@@ -729,7 +729,7 @@ struct BatchItem {
 // they keep the kernel at its 128-register bound, and the stages of one
 // 256^3 solve in a pool take 6-8 % longer (a launch with more solves keeps
 // that path).
-constexpr int BATCH_PARAM_SOLVES = 72;
+constexpr int BATCH_PARAM_SOLVES = 60;
 struct BatchArgs {
   StageArgs a[BATCH_PARAM_SOLVES];
 };

@@ -73,6 +73,27 @@ def test_host_run_and_restart(gpu, tmp_path):
     np.testing.assert_array_equal(psi2, s.get_state())
 
 
+def test_host_pade_pulse_run(gpu, tmp_path):
+    # an ic.in that asks for a Pade rarefaction pulse times the vortex pair
+    # (src/ic.f90:518-636): the host builds it on the device; the end state
+    # equals the Python interface's solve from the same device IC, and the
+    # CPU oracle from the host restatement of the IC
+    d = tmp_path / "run"
+    shutil.copytree(INPUTS / "ring64", d)
+    (d / "ic.in").write_text("  init_cond = pade_pulse_ring('pulse', 1.5_pr, -0.5_pr, 0.5_pr, 0.0_pr) * vortex_pair()\n")
+    run(d)
+    p, t, _, _, psi = read_end_state(d / "proc0000" / "end_state.dat")
+    assert p == 10
+    pulse = dict(x0=1.5, y0=-0.5, z0=0.5, r0=0.0)
+    s = Solver(RP)
+    s.set_ic(ic.device_spec("pade_pulse", "vortex_pair", pulse=pulse))
+    s.solver(10)
+    np.testing.assert_array_equal(psi, s.get_state())
+    psi0 = ic.pade_pulse_ring(RP, "pulse", **pulse) * ic.vortex_pair(RP)
+    ref = Oracle(RP).run(psi0, 10)
+    assert np.linalg.norm(psi - ref) / np.linalg.norm(ref) <= 1e-12
+
+
 def test_host_rejects_existing_end_state(gpu, tmp_path):
     d = tmp_path / "run"
     shutil.copytree(INPUTS / "ring64", d)
