@@ -123,3 +123,24 @@ def test_pool_continuous_batching(gpu):
         out, _ = run_alone_handle(rp, state(rp, seed), n)
         np.testing.assert_array_equal(res[tag].psi, out)
     assert res[2].start_s >= res[2].submit_s
+
+
+@pytest.mark.parametrize("storage, scheme", [("c64", "rk4"), ("c128", "rk4"), ("c64", "rk45"), ("c128", "rk45")])
+def test_classes_beyond_the_parameter_space(gpu, storage, scheme):
+    # a launch carries the stage arguments of up to 60 solves in its
+    # parameter space; a class of 64 solves takes the device-table path.
+    # Both give each solve's states bitwise as the single-solve handle
+    # does (one class of 64 and one of 7 solves in the same pool).
+    steps = 4 if scheme == "rk4" else 3
+    rps = [params((8 + (k % 3), 8, 6 + (k % 2)), 1 + (k % 2), 4, scheme=scheme, storage=storage) for k in range(64)]
+    rps += [params((10, 9, 8), 2, 2, scheme=scheme, storage=storage) for _ in range(7)]
+    pool = Pool(sum(Pool.solve_bytes(rp) for rp in rps) + (64 << 20))
+    psis = [state(rp, k) for k, rp in enumerate(rps)]
+    for k, (rp, psi) in enumerate(zip(rps, psis)):
+        assert pool.submit(rp, psi, steps, k)
+    res = {r.tag: r for r in pool.run_all()}
+    pool.close()
+    for k in (0, 1, 2, 5, 33, 63, 64, 70):
+        alone, s = run_alone_handle(rps[k], psis[k], steps)
+        s.close()
+        np.testing.assert_array_equal(res[k].psi, alone, err_msg=f"solve {k}")
