@@ -255,9 +255,13 @@ int batch_rows(int cmode, int fam) {
   }
 }
 
-int grid_for(int cls, int kind, int nitems) {
+// Persistent grid of a class's launch: as many CTAs as fit on the device at
+// once (of the kernel variant its ns solves select), at most one per item.
+int grid_for(int cls, int kind, int nitems, int ns) {
   int occ = 0;
-  launch_batch(cls, kind, 0, nullptr, BatchLaunch{}, &occ);
+  BatchLaunch q{};
+  q.ns = ns;
+  launch_batch(cls, kind, 0, nullptr, q, &occ);
   return std::max(1, std::min(nitems, occ));
 }
 
@@ -477,7 +481,7 @@ int rk4_enqueue(gpe_pool* P, int cm, int64_t chunk) {
     PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)5 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
     const int kinds[4] = {K_RK4_1, K_RK4_2, K_RK4_3, K_RK4_4};
     int grids[4];
-    for (int m = 0; m < 4; ++m) grids[m] = grid_for(cm, kinds[m], c.nitems);
+    for (int m = 0; m < 4; ++m) grids[m] = grid_for(cm, kinds[m], c.nitems, ns);
     PCU(P, cudaStreamSynchronize(c.st));
     if (int rc = capture_rk4_step(P, c, cm, ns, grids, false, &c.graph, &c.gexec)) return rc;
     if (int rc = capture_rk4_step(P, c, cm, ns, grids, true, &c.graph_n, &c.gexec_n)) return rc;
@@ -534,7 +538,7 @@ int rk45_enqueue(gpe_pool* P, int cm, std::vector<Solve*>& sv) {
   PCU(P, cudaMemcpyAsync(c.tab.p, c.htab.p, (size_t)6 * ns * sizeof(BatchStage), cudaMemcpyHostToDevice, c.st));
   PCU(P, cudaMemsetAsync(c.queue.p, 0, 6 * sizeof(int), c.st));
   for (int m = 0; m < 6; ++m)
-    PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems), c.st,
+    PCU(P, launch_batch(cm, K_CK_1 + m, grid_for(cm, K_CK_1 + m, c.nitems, ns), c.st,
                         BatchLaunch{c.tab.p + (size_t)m * ns, c.htab.p + (size_t)m * ns, ns, c.items.p, c.order.p,
                                     c.nitems, c.queue.p + m, m == 5 ? c.part.p : nullptr},
                         nullptr));

@@ -240,21 +240,32 @@ static cudaError_t launch_batch_one(int grid, cudaStream_t st, const BatchLaunch
   return cudaGetLastError();
 }
 
+// CTAs of the kernel launch_batch_one would launch for b that fit on the
+// device at once (b.ns picks the parameter-space or the table kernel).
+template <class S, class C, int K, int TY, bool PAIR, int RR>
+static cudaError_t batch_occupancy(const BatchLaunch& b, int* occupancy) {
+  constexpr bool kParamArgs = !(sizeof(C) == sizeof(float) && K >= K_CK_1 && K <= K_CK_6);
+  if constexpr (kParamArgs) {
+    if (b.ns >= 1 && b.ns <= BATCH_PARAM_SOLVES) return batch_setup<S, C, K, TY, PAIR, RR, true>(occupancy);
+  }
+  return batch_setup<S, C, K, TY, PAIR, RR, false>(occupancy);
+}
+
 template <class S, class C, int K, int RR>
 static cudaError_t launch_batch_kind_r(int grid, cudaStream_t st, const BatchLaunch& b, int* occupancy) {
   if constexpr (std::is_same<S, float2>::value && std::is_same<C, float>::value) {
     if constexpr (is_rk4_kind(K)) {
       if (batch_rk4_f32_rows() == 16) {
-        if (grid <= 0) return batch_setup<S, C, K, 16, true, RR>(occupancy);
+        if (grid <= 0) return batch_occupancy<S, C, K, 16, true, RR>(b, occupancy);
         return launch_batch_one<S, C, K, 16, true, RR>(grid, st, b);
       }
     }
     if (batch_pair_layout()) {
-      if (grid <= 0) return batch_setup<S, C, K, 8, true, RR>(occupancy);
+      if (grid <= 0) return batch_occupancy<S, C, K, 8, true, RR>(b, occupancy);
       return launch_batch_one<S, C, K, 8, true, RR>(grid, st, b);
     }
   }
-  if (grid <= 0) return batch_setup<S, C, K, 8, false, RR>(occupancy);
+  if (grid <= 0) return batch_occupancy<S, C, K, 8, false, RR>(b, occupancy);
   return launch_batch_one<S, C, K, 8, false, RR>(grid, st, b);
 }
 
