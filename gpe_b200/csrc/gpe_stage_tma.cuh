@@ -181,7 +181,11 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
 // bookkeeping are shared by PY sites.  Returns false when a bounded wait
 // expired (the caller must stop; the copies this item issued have been
 // drained and a.status set).
-template <class S, class C, int R, int KIND, int TY, int PY, class LY>
+// ZU: unroll factor of the z march.  The single-solve kernels take 2 (the
+// z queue shifts are renamed across each pair of planes: +0.8 % complex64,
+// +1.2 % complex128 at 256^3); the persistent batched kernel keeps 1 (its
+// doubled body cost 1 % on the uneven batch).
+template <class S, class C, int R, int KIND, int TY, int PY, class LY, int ZU = 1>
 __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                          TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                          double& r_err) {
@@ -293,6 +297,7 @@ __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a
   int sc_s = (SB + R) % NSS;
   int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
 
+#pragma unroll ZU
   for (int m = 0; m < M; ++m) {
     const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
@@ -407,7 +412,7 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item<S, C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+  if (!tma_item<S, C, R, KIND, TY, PY, LY, 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
                                            r_en, r_err))
     return;
   if (a.partials) block_reduce_store<32 * TY / PY>(r_norm, r_en, r_err, a.partials);
@@ -434,7 +439,7 @@ __device__ __forceinline__ void st_pair(float2* p, float2 v0, float2 v1, bool ac
     *p = v0;
 }
 
-template <class C, int R, int KIND, int TY, int PY, class LY>
+template <class C, int R, int KIND, int TY, int PY, class LY, int ZU = 1>
 __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                               TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
                                               double& r_err) {
@@ -544,6 +549,7 @@ __device__ __forceinline__ bool tma_item_pair(const TmaMaps& maps, const StageAr
   int sc_s = (SB + R) % NSS;
   int pw_s = PB % NPS, pw_p = (PB / NPS) & 1;
 
+#pragma unroll ZU
   for (int m = 0; m < M; ++m) {
     const int k = kb + m;
     const int lc = m + R, ll = m + 2 * R;
@@ -694,7 +700,7 @@ __global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_co
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item_pair<C, R, KIND, TY, PY, LY>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+  if (!tma_item_pair<C, R, KIND, TY, PY, LY, 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
                                              r_en, r_err))
     return;
   if (a.partials) block_reduce_store<16 * TY / PY>(r_norm, r_en, r_err, a.partials);
