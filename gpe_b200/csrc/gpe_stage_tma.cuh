@@ -181,10 +181,11 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
 // bookkeeping are shared by PY sites.  Returns false when a bounded wait
 // expired (the caller must stop; the copies this item issued have been
 // drained and a.status set).
-// ZU: unroll factor of the z march.  The single-solve kernels take 2 (the
-// z queue shifts are renamed across each pair of planes: +0.8 % complex64,
-// +1.2 % complex128 at 256^3); the persistent batched kernel keeps 1 (its
-// doubled body cost 1 % on the uneven batch).
+// ZU: unroll factor of the z march (the z-queue shifts are renamed across
+// ZU planes).  At 256^3, 2 against 1: +0.7 % complex64 (pair kernel),
+// +1.2 % complex128; 3 against 2: -0.9 % complex64, +0.5 % complex128.
+// The single-solve kernels take 3 for complex128 sites and 2 otherwise;
+// the persistent batched kernel keeps 1 (2 cost 1 % on the uneven batch).
 template <class S, class C, int R, int KIND, int TY, int PY, class LY, int ZU = 1>
 __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                          TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
@@ -412,7 +413,8 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item<S, C, R, KIND, TY, PY, LY, 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+  if (!tma_item<S, C, R, KIND, TY, PY, LY, sizeof(S) == 16 ? 3 : 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg,
+                                                                    &s_abort, r_norm,
                                            r_en, r_err))
     return;
   if (a.partials) block_reduce_store<32 * TY / PY>(r_norm, r_en, r_err, a.partials);
