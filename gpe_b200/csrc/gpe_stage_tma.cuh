@@ -181,11 +181,20 @@ __device__ __forceinline__ TmaRing tma_ring_setup(unsigned char* smem_raw, int* 
 // bookkeeping are shared by PY sites.  Returns false when a bounded wait
 // expired (the caller must stop; the copies this item issued have been
 // drained and a.status set).
+// Unroll factor of the single-solve kernels' z march.  RK4 stages at
+// 256^3, 2 against 1: +0.7 % complex64 (pair kernel), +1.2 % complex128;
+// 3 against 2: -0.9 % complex64, +0.5 % complex128.  The Cash-Karp stages
+// of the 192^2 x 384 RKF45 solve lose 1.5 % with 3 (complex128), so the
+// other schemes keep 1, as does the persistent batched kernel (2 cost 1 %
+// on the uneven batch).
+template <class S, int KIND>
+__host__ __device__ constexpr int single_zu() {
+  return (KIND == K_RK4_1 || KIND == K_RK4_2 || KIND == K_RK4_3 || KIND == K_RK4_4) ? (sizeof(S) == 16 ? 3 : 2)
+                                                                                     : 1;
+}
+
 // ZU: unroll factor of the z march (the z-queue shifts are renamed across
-// ZU planes).  At 256^3, 2 against 1: +0.7 % complex64 (pair kernel),
-// +1.2 % complex128; 3 against 2: -0.9 % complex64, +0.5 % complex128.
-// The single-solve kernels take 3 for complex128 sites and 2 otherwise;
-// the persistent batched kernel keeps 1 (2 cost 1 % on the uneven batch).
+// ZU planes); see single_zu.
 template <class S, class C, int R, int KIND, int TY, int PY, class LY, int ZU = 1>
 __device__ __forceinline__ bool tma_item(const TmaMaps& maps, const StageArgs& a, int bx, int by, int bz,
                                          TmaRing& rg, int* s_abort, double& r_norm, double& r_en,
@@ -413,8 +422,8 @@ __global__ void __launch_bounds__(32 * TY / PY) k_stage_tma(const __grid_constan
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item<S, C, R, KIND, TY, PY, LY, sizeof(S) == 16 ? 3 : 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg,
-                                                                    &s_abort, r_norm,
+  if (!tma_item<S, C, R, KIND, TY, PY, LY, single_zu<S, KIND>()>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg,
+                                                                  &s_abort, r_norm,
                                            r_en, r_err))
     return;
   if (a.partials) block_reduce_store<32 * TY / PY>(r_norm, r_en, r_err, a.partials);
@@ -702,7 +711,8 @@ __global__ void __launch_bounds__(16 * TY / PY) k_stage_tma_pair(const __grid_co
   __shared__ int s_abort;
   TmaRing rg = tma_ring_setup<LY>(smem_raw, &s_abort);
   double r_norm = 0.0, r_en = 0.0, r_err = 0.0;
-  if (!tma_item_pair<C, R, KIND, TY, PY, LY, 2>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z, rg, &s_abort, r_norm,
+  if (!tma_item_pair<C, R, KIND, TY, PY, LY, single_zu<float2, KIND>()>(maps, a, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                                       rg, &s_abort, r_norm,
                                              r_en, r_err))
     return;
   if (a.partials) block_reduce_store<16 * TY / PY>(r_norm, r_en, r_err, a.partials);
